@@ -1,0 +1,851 @@
+// The C-ABI of include/gdon3d_cuda.h: handle life cycle, attach (setup on the
+// device), the time loops, state conversion and norms.  Host orchestration
+// only; the arithmetic is in rk3.cu, kinetic.cu and aux.cu.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "aux.h"
+#include "kernels.h"
+
+namespace gdn {
+template <typename GT>
+int launch_kin_setup(const int *face2elem, long long nf, const double *geom, const int *nb, long long ne,
+					 const KinModel &km, double theta_dt, GT *sown, double *sown64, unsigned char *mask, GT *G,
+					 GT *coef, int *bad, cudaStream_t s);
+}
+
+using namespace gdn;
+
+// ---------------------------------------------------------------- errors --
+static thread_local std::string g_last_error;
+
+int gdn_set_error(int code, const char *msg)
+{
+	g_last_error = msg ? msg : "";
+	return code;
+}
+
+int gdn_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
+{
+	char buf[512];
+	std::snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what,
+				  file, line);
+	g_last_error = buf;
+	return e == cudaErrorMemoryAllocation ? GDN_CUDA_ERR_OOM : GDN_CUDA_ERR_CUDA;
+}
+
+extern "C" const char *gdn_cuda_last_error(void)
+{
+	return g_last_error.c_str();
+}
+
+#define GDN_TRY(expr)                                                                              \
+	do {                                                                                           \
+		int _rc = (expr);                                                                          \
+		if (_rc != GDN_CUDA_OK)                                                                    \
+			return _rc;                                                                            \
+	} while (0)
+
+// ---------------------------------------------------------------- handle --
+struct DevBuf {
+	void *p = nullptr;
+	size_t bytes = 0;
+};
+
+struct gdn_cuda_handle {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	int scheme = 0, precision = 0, nv = 0, use_graph = 1;
+	long long ne = 0, nf = 0, nbf = 0, nq = 0, neq = 0;
+	double dt = 0, theta = 0.5, omega = 0, lambda = 0;
+	Data data{};
+	KinModel km{};
+	double t = 0; // current time (host copy, accumulated like the reference)
+	double t_bdof = 0; // RK3: time of the boundary data of the last stage
+	long long steps = 0;
+	long long launches = 0;
+	int ssize = 8; // bytes per stored state value
+	// device arrays
+	std::vector<DevBuf> bufs;
+	int *e2q = nullptr;
+	double *node = nullptr;
+	double *geom64 = nullptr;
+	void *geomT = nullptr;
+	int *nb = nullptr;
+	int *perm = nullptr;
+	int *face2elem = nullptr;
+	double *bxyz = nullptr;
+	double *partial = nullptr;
+	double *result = nullptr; // [7]
+	double *staging = nullptr; // m * neq doubles (reference layout)
+	int *flag = nullptr;
+	double *host_result = nullptr; // pinned [8]
+	int nblk_err = 0;
+	// RK3
+	void *w[2] = {nullptr, nullptr};
+	void *k2 = nullptr;
+	int cur = 0;
+	// kinetic
+	void *f = nullptr, *y = nullptr, *G = nullptr, *sown = nullptr, *coef = nullptr;
+	int *items = nullptr;
+	std::vector<int> level_off;
+};
+
+template <typename X>
+static int dalloc(gdn_cuda_handle *h, X **p, size_t count)
+{
+	void *q = nullptr;
+	const size_t bytes = count * sizeof(X) > 0 ? count * sizeof(X) : 16;
+	cudaError_t e = cudaMalloc(&q, bytes);
+	if (e != cudaSuccess) {
+		cudaGetLastError();
+		char buf[160];
+		std::snprintf(buf, sizeof(buf), "device allocation of %zu bytes failed", bytes);
+		return gdn_set_error(GDN_CUDA_ERR_OOM, buf);
+	}
+	DevBuf b;
+	b.p = q;
+	b.bytes = bytes;
+	h->bufs.push_back(b);
+	*p = reinterpret_cast<X *>(q);
+	return GDN_CUDA_OK;
+}
+
+static void free_handle(gdn_cuda_handle *h)
+{
+	if (!h)
+		return;
+	cudaSetDevice(h->device);
+	if (h->stream)
+		cudaStreamSynchronize(h->stream);
+	for (auto &b : h->bufs)
+		cudaFree(b.p);
+	if (h->host_result)
+		cudaFreeHost(h->host_result);
+	if (h->stream)
+		cudaStreamDestroy(h->stream);
+	delete h;
+}
+
+// -------------------------------------------------------- table upload --
+template <typename T>
+static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
+{
+	std::memset(&o, 0, sizeof(o));
+	for (int k = 0; k < 3; k++)
+		for (int i = 0; i < 10; i++)
+			for (int j = 0; j < 10; j++)
+				o.D[k][i][j] = (T)t->internal[i][j][k];
+	for (int i = 0; i < 10; i++) {
+		o.wpg[i] = (T)t->wpg[i];
+		for (int j = 0; j < 10; j++) {
+			o.Minv[i][j] = (T)t->inv_mass[i][j];
+			o.M[i][j] = (T)t->mass[i][j];
+		}
+	}
+	for (int i = 0; i < 6; i++)
+		for (int j = 0; j < 6; j++)
+			o.S[i][j] = (T)t->face_scal[i][j];
+	for (int f = 0; f < 4; f++) {
+		for (int k = 0; k < 3; k++)
+			o.ref_normal[f][k] = t->ref_normal[f][k];
+		for (int j = 0; j < 6; j++)
+			o.f2n[f][j] = t->face2node[f][j];
+	}
+	for (int i = 0; i < 10; i++)
+		o.nface_of_node[i] = 0;
+	for (int f = 0; f < 4; f++)
+		for (int j = 0; j < 6; j++) {
+			const int i = t->face2node[f][j];
+			const int a = o.nface_of_node[i]++;
+			if (a < 3) {
+				o.face_of_node[i][a] = f;
+				o.pos_of_node[i][a] = j;
+			}
+		}
+}
+
+static int upload_tables(const gdn_cuda_tables *t)
+{
+	for (int f = 0; f < 4; f++)
+		for (int j = 0; j < 6; j++)
+			if (t->face2node[f][j] < 0 || t->face2node[f][j] > 9)
+				return gdn_set_error(GDN_CUDA_ERR_INVALID, "tables: face2node out of range");
+	Tables<double> td;
+	Tables<float> tf;
+	fill_tables(t, td);
+	fill_tables(t, tf);
+	for (int i = 0; i < 10; i++)
+		if (td.nface_of_node[i] < 2 || td.nface_of_node[i] > 3)
+			return gdn_set_error(GDN_CUDA_ERR_INVALID, "tables: face2node does not cover the P2 nodes");
+	GDN_CUDA_TRY(cudaMemcpyToSymbol(c_tab_d, &td, sizeof(td)));
+	GDN_CUDA_TRY(cudaMemcpyToSymbol(c_tab_f, &tf, sizeof(tf)));
+	return GDN_CUDA_OK;
+}
+
+// ------------------------------------------------------------ attach --
+static int validate_mesh(const gdn_cuda_mesh *m)
+{
+	if (!m || m->nbelems <= 0 || m->nbfaces <= 0 || m->nboundaryfaces < 0 || m->nbqnodes <= 0 ||
+		!m->face2elem || !m->fnode2enode || !m->elem2qnode || !m->node ||
+		(m->nboundaryfaces > 0 && !m->boundaryface))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: mesh arrays or sizes missing");
+	const long long ne = m->nbelems, nf = m->nbfaces;
+	for (long long i = 0; i < 10 * ne + 6LL * m->nboundaryfaces; i++)
+		if (m->elem2qnode[i] < 0 || m->elem2qnode[i] >= m->nbqnodes)
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: elem2qnode index out of range");
+	long long nbf = 0;
+	for (long long F = 0; F < nf; F++) {
+		const int eL = m->face2elem[4 * F], fL = m->face2elem[4 * F + 1], eR = m->face2elem[4 * F + 2],
+				  fR = m->face2elem[4 * F + 3];
+		if (eL < 0 || eL >= ne || fL < 0 || fL > 3 || eR >= ne || (eR >= 0 && (fR < 0 || fR > 3)))
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: face2elem entry out of range");
+		if (eR < 0)
+			nbf++;
+	}
+	if (nbf != m->nboundaryfaces)
+		return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: nboundaryfaces does not match face2elem");
+	return GDN_CUDA_OK;
+}
+
+static int validate_data(const gdn_cuda_data *d)
+{
+	if (!d || (d->kind != GDN_CUDA_DATA_PLANE && d->kind != GDN_CUDA_DATA_CAVITY))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown analytic data kind");
+	if (d->kind == GDN_CUDA_DATA_PLANE) {
+		const double kk = d->khat[0] * d->khat[0] + d->khat[1] * d->khat[1] + d->khat[2] * d->khat[2];
+		const double kp = d->khat[0] * d->pol[0] + d->khat[1] * d->pol[1] + d->khat[2] * d->pol[2];
+		if (!(std::fabs(kk - 1.0) < 1e-12) || !(std::fabs(kp) < 1e-12) || !std::isfinite(d->kmag) ||
+			!std::isfinite(d->amp) || !std::isfinite(d->phase))
+			return gdn_set_error(GDN_CUDA_ERR_INVALID,
+								 "attach: plane wave needs a unit direction and a polarisation orthogonal to it");
+	}
+	return GDN_CUDA_OK;
+}
+
+// neighbour / permutation / boundary tables from face2elem + fnode2enode
+static int build_neighbours(const gdn_cuda_mesh *m, const gdn_cuda_tables *t, std::vector<int> &nb,
+							std::vector<int> &perm, std::vector<double> &bxyz)
+{
+	const long long ne = m->nbelems, nf = m->nbfaces, nbf = m->nboundaryfaces;
+	nb.assign(4 * ne, INT32_MIN);
+	perm.assign(4 * ne, 0);
+	bxyz.assign(nbf * 18, 0.0);
+	std::vector<long long> bidx(nf, -1);
+	for (long long b = 0; b < nbf; b++) {
+		const int F = m->boundaryface[b];
+		if (F < 0 || F >= nf || m->face2elem[4LL * F + 2] >= 0)
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: boundaryface lists a non-boundary face");
+		bidx[F] = b;
+	}
+	for (long long F = 0; F < nf; F++) {
+		const int eL = m->face2elem[4 * F], fL = m->face2elem[4 * F + 1], eR = m->face2elem[4 * F + 2],
+				  fR = m->face2elem[4 * F + 3];
+		const int *fn = m->fnode2enode + 12 * F;
+		for (int j = 0; j < 6; j++)
+			if (fn[j] != t->face2node[fL][j])
+				return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: fnode2enode (L side) disagrees with face2node");
+		if (nb[4LL * eL + fL] != INT32_MIN)
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: element face listed twice");
+		if (eR < 0) {
+			const long long b = bidx[F];
+			if (b < 0)
+				return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: boundary face missing from boundaryface");
+			nb[4LL * eL + fL] = (int)(-(b + 1));
+			for (int j = 0; j < 6; j++) {
+				const long long q = m->elem2qnode[10LL * eL + fn[j]];
+				for (int c = 0; c < 3; c++)
+					bxyz[(b * 6 + j) * 3 + c] = m->node[3 * q + c];
+			}
+			continue;
+		}
+		if (nb[4LL * eR + fR] != INT32_MIN)
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: element face listed twice");
+		nb[4LL * eL + fL] = eR;
+		nb[4LL * eR + fR] = eL;
+		int pL = 0, pR = 0;
+		for (int j = 0; j < 6; j++) {
+			const int qr = fn[6 + j];
+			if (qr < 0 || qr > 9)
+				return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: fnode2enode (R side) out of range");
+			pL |= qr << (4 * j);
+		}
+		for (int j = 0; j < 6; j++) {
+			const int qself = t->face2node[fR][j];
+			int jj = 0;
+			while (jj < 6 && fn[6 + jj] != qself)
+				jj++;
+			if (jj == 6)
+				return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: faces of neighbours do not match");
+			pR |= fn[jj] << (4 * j);
+		}
+		perm[4LL * eL + fL] = pL;
+		perm[4LL * eR + fR] = pR;
+	}
+	for (long long i = 0; i < 4 * ne; i++)
+		if (nb[i] == INT32_MIN)
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: an element face has no face record");
+	return GDN_CUDA_OK;
+}
+
+// host Kahn scheduling of the upwind DAG per velocity; items grouped by level
+static int build_schedule(gdn_cuda_handle *h, const std::vector<unsigned char> &mask,
+						  const std::vector<int> &nbv, std::vector<int> &items, std::vector<int> &off)
+{
+	const long long ne = h->ne;
+	const int nv = h->nv;
+	std::vector<int> level(ne * nv, 0);
+	std::vector<int> indeg(ne);
+	std::vector<long long> queue(ne);
+	int maxlev = 0;
+	for (int v = 0; v < nv; v++) {
+		long long qh = 0, qt = 0;
+		for (long long e = 0; e < ne; e++) {
+			const unsigned char mk = mask[e * nv + v];
+			indeg[e] = __builtin_popcount(mk);
+			level[e * nv + v] = 0;
+			if (indeg[e] == 0)
+				queue[qt++] = e;
+		}
+		while (qh < qt) {
+			const long long e = queue[qh++];
+			const int le = level[e * nv + v];
+			for (int f = 0; f < 4; f++) {
+				const int d = nbv[4 * e + f];
+				if (d < 0)
+					continue;
+				// d depends on e iff d's mask has the face that points to e
+				const unsigned char md = mask[(long long)d * nv + v];
+				bool dep = false;
+				for (int g = 0; g < 4; g++)
+					if ((md >> g & 1) && nbv[4LL * d + g] == e)
+						dep = true;
+				if (!dep)
+					continue;
+				if (level[(long long)d * nv + v] < le + 1)
+					level[(long long)d * nv + v] = le + 1;
+				if (--indeg[d] == 0)
+					queue[qt++] = d;
+			}
+		}
+		if (qt != ne)
+			return gdn_set_error(GDN_CUDA_ERR_CYCLE, "attach: the upwind element graph has a cycle");
+		for (long long e = 0; e < ne; e++)
+			if (level[e * nv + v] > maxlev)
+				maxlev = level[e * nv + v];
+	}
+	const int nl = maxlev + 1;
+	off.assign(nl + 1, 0);
+	for (long long u = 0; u < ne * nv; u++)
+		off[level[u] + 1]++;
+	for (int l = 0; l < nl; l++)
+		off[l + 1] += off[l];
+	items.assign(ne * nv, 0);
+	std::vector<int> pos(off.begin(), off.end() - 1);
+	for (long long u = 0; u < ne * nv; u++)
+		items[pos[level[u]]++] = (int)u;
+	return GDN_CUDA_OK;
+}
+
+template <typename S>
+static S *as(void *p)
+{
+	return reinterpret_cast<S *>(p);
+}
+
+static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cuda_tables *t,
+					   const gdn_cuda_model *mo)
+{
+	const long long ne = h->ne, nf = h->nf, nbf = h->nbf;
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	GDN_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+	GDN_TRY(upload_tables(t));
+	std::vector<int> nb, perm;
+	std::vector<double> bx;
+	GDN_TRY(build_neighbours(m, t, nb, perm, bx));
+
+	GDN_TRY(dalloc(h, &h->e2q, 10 * ne));
+	GDN_TRY(dalloc(h, &h->node, 3 * h->nq));
+	GDN_TRY(dalloc(h, &h->geom64, 10 * ne));
+	GDN_TRY(dalloc(h, &h->nb, 4 * ne));
+	GDN_TRY(dalloc(h, &h->perm, 4 * ne));
+	GDN_TRY(dalloc(h, &h->face2elem, 4 * nf));
+	GDN_TRY(dalloc(h, &h->bxyz, 18 * (nbf > 0 ? nbf : 1)));
+	GDN_TRY(dalloc(h, &h->flag, 4));
+	h->nblk_err = 1184; // 8 x 148 SMs
+	GDN_TRY(dalloc(h, &h->partial, 6 * h->nblk_err));
+	GDN_TRY(dalloc(h, &h->result, 8));
+	GDN_CUDA_TRY(cudaMallocHost(&h->host_result, 8 * sizeof(double)));
+	cudaStream_t s = h->stream;
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->e2q, m->elem2qnode, 10 * ne * sizeof(int), cudaMemcpyHostToDevice, s));
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->node, m->node, 3 * h->nq * sizeof(double), cudaMemcpyHostToDevice, s));
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->nb, nb.data(), 4 * ne * sizeof(int), cudaMemcpyHostToDevice, s));
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->perm, perm.data(), 4 * ne * sizeof(int), cudaMemcpyHostToDevice, s));
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->face2elem, m->face2elem, 4 * nf * sizeof(int), cudaMemcpyHostToDevice, s));
+	if (nbf > 0)
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->bxyz, bx.data(), 18 * nbf * sizeof(double), cudaMemcpyHostToDevice, s));
+	GDN_CUDA_TRY(cudaMemsetAsync(h->flag, 0, 4 * sizeof(int), s));
+	GDN_TRY(launch_geometry(h->e2q, h->node, ne, h->geom64, h->flag, s));
+	h->launches++;
+	int bad = 0;
+	GDN_CUDA_TRY(cudaMemcpyAsync(&bad, h->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+	GDN_CUDA_TRY(cudaStreamSynchronize(s));
+	if (bad)
+		return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: an element has a non-positive Jacobian determinant");
+
+	const bool fp64 = h->precision == GDN_CUDA_FP64;
+	if (fp64) {
+		h->geomT = h->geom64;
+	} else {
+		float *g32;
+		GDN_TRY(dalloc(h, &g32, 10 * ne));
+		GDN_TRY(launch_convert<float>(h->geom64, g32, 10 * ne, s));
+		h->launches++;
+		h->geomT = g32;
+	}
+
+	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+		h->neq = 10 * ne + 6 * nbf;
+		GDN_TRY(prepare_rk3<double>());
+		GDN_TRY(prepare_rk3<float>());
+		for (int b = 0; b < 2; b++) {
+			if (fp64)
+				GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->w[b]), 60 * ne));
+			else
+				GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->w[b]), 60 * ne));
+		}
+		if (fp64)
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->k2), 60 * ne));
+		else
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->k2), 60 * ne));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * ne * h->ssize, s));
+		GDN_TRY(dalloc(h, &h->staging, 6 * h->neq));
+	} else {
+		const int nv = h->nv;
+		h->neq = 10 * ne + 6 * nbf;
+		double *sown64;
+		unsigned char *mask;
+		GDN_TRY(dalloc(h, &sown64, 4 * ne * nv));
+		GDN_TRY(dalloc(h, &mask, ne * nv));
+		if (fp64) {
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->G), 100 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->sown), 4 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->coef), ne));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->y), 60 * ne * nv));
+			GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->theta * h->dt,
+											 as<double>(h->sown), sown64, mask, as<double>(h->G),
+											 as<double>(h->coef), h->flag, s));
+		} else {
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->G), 100 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->sown), 4 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->coef), ne));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->f), 60 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->y), 60 * ne * nv));
+			GDN_TRY(launch_kin_setup<float>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->theta * h->dt,
+											as<float>(h->sown), sown64, mask, as<float>(h->G), as<float>(h->coef),
+											h->flag, s));
+		}
+		h->launches += 3;
+		std::vector<unsigned char> hmask(ne * nv);
+		GDN_CUDA_TRY(cudaMemcpyAsync(hmask.data(), mask, ne * nv, cudaMemcpyDeviceToHost, s));
+		GDN_CUDA_TRY(cudaMemcpyAsync(&bad, h->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+		GDN_CUDA_TRY(cudaStreamSynchronize(s));
+		if (bad)
+			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: a transport diagonal block is singular");
+		std::vector<int> items;
+		GDN_TRY(build_schedule(h, hmask, nb, items, h->level_off));
+		GDN_TRY(dalloc(h, &h->items, items.size()));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->items, items.data(), items.size() * sizeof(int), cudaMemcpyHostToDevice,
+									 s));
+		GDN_TRY(dalloc(h, &h->staging, (long long)6 * nv * h->neq));
+		GDN_CUDA_TRY(cudaStreamSynchronize(s));
+	}
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
+							   const gdn_cuda_model *model, const gdn_cuda_data *data,
+							   const gdn_cuda_config *config, double dt, gdn_cuda_handle **out)
+{
+	if (!out)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: out is NULL");
+	*out = nullptr;
+	if (!tables || !model)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: tables or model missing");
+	GDN_TRY(validate_mesh(mesh));
+	GDN_TRY(validate_data(data));
+	if (!(dt > 0.0) || !std::isfinite(dt))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: dt must be positive");
+	if (model->nb_w != 6)
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: only Maxwell (nb_w = 6) runs on the device");
+	if (model->scheme != GDN_CUDA_SCHEME_RK3 && model->scheme != GDN_CUDA_SCHEME_KINETIC)
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: unknown scheme");
+	gdn_cuda_config cfg = {GDN_CUDA_FP64, 1, 0, 1, 0};
+	if (config)
+		cfg = *config;
+	if (cfg.precision < GDN_CUDA_FP64 || cfg.precision > GDN_CUDA_BF16_STORE)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
+	if (model->scheme == GDN_CUDA_SCHEME_RK3 && cfg.precision > GDN_CUDA_FP32)
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: RK3 supports FP64 and FP32");
+	if (model->scheme == GDN_CUDA_SCHEME_KINETIC) {
+		if (model->nb_v != 4 && model->nb_v != 6)
+			return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: kinetic sets d3q4 (4) or d3q6 (6) only");
+		if (!model->vi || !(model->lambda > 0.0) || !(model->theta > 0.0) || !(model->theta <= 1.0))
+			return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kinetic model needs vi, lambda > 0, 0 < theta <= 1");
+		if (cfg.precision > GDN_CUDA_FP32)
+			return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: precision mode not built for the kinetic path");
+	}
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+		cudaGetLastError();
+		return gdn_set_error(GDN_CUDA_ERR_CUDA, "attach: no CUDA device");
+	}
+	if (cfg.device < 0 || cfg.device >= ndev)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: bad device ordinal");
+
+	gdn_cuda_handle *h = new gdn_cuda_handle();
+	h->device = cfg.device;
+	h->scheme = model->scheme;
+	h->precision = cfg.precision;
+	h->use_graph = cfg.use_graph;
+	h->ne = mesh->nbelems;
+	h->nf = mesh->nbfaces;
+	h->nbf = mesh->nboundaryfaces;
+	h->nq = mesh->nbqnodes;
+	h->dt = dt;
+	h->theta = model->theta > 0 ? model->theta : 0.5;
+	h->omega = model->omega;
+	h->lambda = model->lambda;
+	h->ssize = cfg.precision == GDN_CUDA_FP64 ? 8 : 4;
+	h->data.kind = data->kind;
+	for (int c = 0; c < 3; c++) {
+		h->data.khat[c] = data->khat[c];
+		h->data.pol[c] = data->pol[c];
+	}
+	h->data.kmag = data->kmag;
+	h->data.amp = data->amp;
+	h->data.phase = data->phase;
+	if (h->scheme == GDN_CUDA_SCHEME_KINETIC) {
+		h->nv = model->nb_v;
+		h->km.nv = h->nv;
+		for (int i = 0; i < 3 * h->nv; i++)
+			h->km.vi[i] = model->vi[i];
+		const double l2 = model->lambda * model->lambda;
+		h->km.feq_c = h->nv == 4 ? 1.0 / (4.0 * l2) : 1.0 / (2.0 * l2);
+	}
+	int rc = attach_impl(h, mesh, tables, model);
+	if (rc != GDN_CUDA_OK) {
+		std::string msg = g_last_error;
+		free_handle(h);
+		g_last_error = msg;
+		return rc;
+	}
+	*out = h;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_detach(gdn_cuda_handle *h)
+{
+	if (!h)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "detach: NULL handle");
+	free_handle(h);
+	return GDN_CUDA_OK;
+}
+
+// ------------------------------------------------------------ stepping --
+static const double RK_A[3] = {0., -5. / 9., -153. / 128.};
+static const double RK_B[3] = {1. / 3., 15. / 16., 8. / 15.};
+static const double RK_C[3] = {0., 1. / 3., 3. / 4.};
+
+template <typename T>
+static int rk3_step(gdn_cuda_handle *h)
+{
+	for (int i = 0; i < 3; i++) {
+		Rk3Params<T> p;
+		p.w_in = as<T>(h->w[h->cur]);
+		p.w_out = as<T>(h->w[1 - h->cur]);
+		p.k2 = as<T>(h->k2);
+		p.geom = reinterpret_cast<const T *>(h->geomT);
+		p.nb = h->nb;
+		p.perm = h->perm;
+		p.bxyz = h->bxyz;
+		p.data = h->data;
+		p.ne = h->ne;
+		p.t_stage = h->t + RK_C[i] * h->dt;
+		p.dt = h->dt;
+		p.A = RK_A[i];
+		p.B = RK_B[i];
+		p.stage0 = i == 0;
+		p.write_k2 = i < 2;
+		GDN_TRY(launch_rk3_stage<T>(p, h->stream));
+		h->launches++;
+		h->cur = 1 - h->cur;
+		h->t_bdof = p.t_stage;
+	}
+	h->t += h->dt;
+	h->steps++;
+	return GDN_CUDA_OK;
+}
+
+template <typename T>
+static int kin_step(gdn_cuda_handle *h)
+{
+	KinSweepParams<T> p;
+	p.f = as<T>(h->f);
+	p.y = as<T>(h->y);
+	p.G = h->G;
+	p.sown = h->sown;
+	p.nb = h->nb;
+	p.perm = h->perm;
+	p.bxyz = h->bxyz;
+	p.coef = h->coef;
+	p.items = h->items;
+	p.data = h->data;
+	p.t_half = h->t + h->dt / 2;
+	for (int i = 0; i < 3 * NV_MAX; i++)
+		p.vi[i] = h->km.vi[i];
+	p.feq_c = h->km.feq_c;
+	p.nv = h->nv;
+	const int nl = (int)h->level_off.size() - 1;
+	for (int l = 0; l < nl; l++) {
+		p.item_begin = h->level_off[l];
+		p.item_end = h->level_off[l + 1];
+		GDN_TRY((launch_kin_sweep<T, T>(p, h->stream)));
+		h->launches++;
+	}
+	KinRelaxParams<T> r;
+	r.f = as<T>(h->f);
+	r.y = as<T>(h->y);
+	r.ne = h->ne;
+	r.nv = h->nv;
+	for (int i = 0; i < 3 * NV_MAX; i++)
+		r.vi[i] = h->km.vi[i];
+	r.feq_c = h->km.feq_c;
+	r.omega = h->omega;
+	r.a_y = 1.0 / h->theta;
+	r.a_f = -(1.0 - h->theta) / h->theta;
+	r.two_over_theta_minus = 0;
+	GDN_TRY(launch_kin_relax<T>(r, h->stream));
+	h->launches++;
+	h->t += h->dt;
+	h->steps++;
+	return GDN_CUDA_OK;
+}
+
+static int advance_impl(gdn_cuda_handle *h, int nsteps)
+{
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	for (int n = 0; n < nsteps; n++) {
+		if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(rk3_step<double>(h));
+			else
+				GDN_TRY(rk3_step<float>(h));
+		} else {
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(kin_step<double>(h));
+			else
+				GDN_TRY(kin_step<float>(h));
+		}
+	}
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_advance(gdn_cuda_handle *h, int nsteps)
+{
+	if (!h || nsteps < 0)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "advance: bad arguments");
+	return advance_impl(h, nsteps);
+}
+
+extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
+{
+	if (!h)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "init: NULL handle");
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	cudaStream_t s = h->stream;
+	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+		h->cur = 0;
+		if (h->precision == GDN_CUDA_FP64)
+			GDN_TRY(launch_init_rk3<double>(h->e2q, h->node, h->ne, h->data, as<double>(h->w[0]), s));
+		else
+			GDN_TRY(launch_init_rk3<float>(h->e2q, h->node, h->ne, h->data, as<float>(h->w[0]), s));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
+	} else {
+		if (h->precision == GDN_CUDA_FP64)
+			GDN_TRY(launch_init_kin<double>(h->e2q, h->node, h->ne, h->data, h->km, as<double>(h->f), s));
+		else
+			GDN_TRY(launch_init_kin<float>(h->e2q, h->node, h->ne, h->data, h->km, as<float>(h->f), s));
+	}
+	h->launches++;
+	h->t = 0.0;
+	h->t_bdof = 0.0;
+	h->steps = 0;
+	return GDN_CUDA_OK;
+}
+
+// reference-layout state -> device (boundary dofs are not state on the
+// device: they are analytic data, re-derived when written back)
+extern "C" int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t)
+{
+	if (!h || !wn)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "set_state: bad arguments");
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	cudaStream_t s = h->stream;
+	const long long ne = h->ne;
+	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+		h->cur = 0;
+		if (h->precision == GDN_CUDA_FP64) {
+			GDN_CUDA_TRY(cudaMemcpyAsync(h->w[0], wn, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
+		} else {
+			GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
+			GDN_TRY(launch_convert<float>(h->staging, as<float>(h->w[0]), 60 * ne, s));
+			h->launches++;
+		}
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * ne * h->ssize, s));
+	} else {
+		const long long wl = (long long)6 * h->nv * h->neq;
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, wl * sizeof(double), cudaMemcpyHostToDevice, s));
+		if (h->precision == GDN_CUDA_FP64)
+			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), ne, h->nv, h->neq, h->staging, 0, s));
+		else
+			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), ne, h->nv, h->neq, h->staging, 0, s));
+		h->launches++;
+	}
+	h->t = t;
+	h->t_bdof = t;
+	return GDN_CUDA_OK;
+}
+
+static int get_state_impl(gdn_cuda_handle *h, double *wn)
+{
+	cudaStream_t s = h->stream;
+	const long long ne = h->ne;
+	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+		double *bd = h->staging + 60 * ne;
+		GDN_TRY(launch_boundary_dofs(h->bxyz, h->nbf, h->data, h->t_bdof, 0, h->km, h->neq, bd, s));
+		h->launches++;
+		if (h->precision == GDN_CUDA_FP64) {
+			GDN_CUDA_TRY(
+				cudaMemcpyAsync(wn, h->w[h->cur], 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
+		} else {
+			GDN_TRY(launch_widen(as<float>(h->w[h->cur]), h->staging, 60 * ne, s));
+			h->launches++;
+			GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
+		}
+		GDN_CUDA_TRY(cudaMemcpyAsync(wn + 60 * ne, bd, 36 * h->nbf * sizeof(double), cudaMemcpyDeviceToHost, s));
+	} else {
+		// boundary dofs after dg_update_boundary(simu, t) (relaxation.c:175)
+		GDN_TRY(launch_boundary_dofs(h->bxyz, h->nbf, h->data, h->t, 1, h->km, h->neq, h->staging + 10 * ne, s));
+		if (h->precision == GDN_CUDA_FP64)
+			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), ne, h->nv, h->neq, h->staging, 1, s));
+		else
+			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), ne, h->nv, h->neq, h->staging, 1, s));
+		h->launches += 2;
+		GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, (long long)6 * h->nv * h->neq * sizeof(double),
+									 cudaMemcpyDeviceToHost, s));
+	}
+	GDN_CUDA_TRY(cudaStreamSynchronize(s));
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_get_state(gdn_cuda_handle *h, double *wn)
+{
+	if (!h || !wn)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "get_state: bad arguments");
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	return get_state_impl(h, wn);
+}
+
+extern "C" int gdn_cuda_step_host(gdn_cuda_handle *h, double *wn, int nsteps)
+{
+	if (!h || !wn || nsteps < 0)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "step_host: bad arguments");
+	GDN_TRY(gdn_cuda_set_state(h, wn, h->t));
+	GDN_TRY(advance_impl(h, nsteps));
+	return get_state_impl(h, wn);
+}
+
+extern "C" int gdn_cuda_solve(gdn_cuda_handle *h, int itermax, double *wn, double *t, double *cpu_running_t)
+{
+	if (!h || !wn || itermax < 0)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "solve: bad arguments");
+	GDN_TRY(gdn_cuda_init(h));
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	auto t0 = std::chrono::steady_clock::now();
+	GDN_TRY(advance_impl(h, itermax));
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	auto t1 = std::chrono::steady_clock::now();
+	GDN_TRY(get_state_impl(h, wn));
+	if (t)
+		*t = h->t;
+	if (cpu_running_t)
+		*cpu_running_t = std::chrono::duration<double>(t1 - t0).count();
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err)
+{
+	if (!h || !err)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "error_l2: bad arguments");
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	cudaStream_t s = h->stream;
+	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
+	const void *st = kin ? h->f : h->w[h->cur];
+	if (h->precision == GDN_CUDA_FP64)
+		GDN_TRY(launch_error_l2<double>(as<double>(const_cast<void *>(st)), kin, h->nv, h->e2q, h->node,
+										h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
+	else
+		GDN_TRY(launch_error_l2<float>(as<float>(const_cast<void *>(st)), kin, h->nv, h->e2q, h->node, h->geom64,
+									   h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
+	h->launches += 2;
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->host_result, h->result, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+	GDN_CUDA_TRY(cudaStreamSynchronize(s));
+	*err = h->host_result[0];
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_get_time(gdn_cuda_handle *h, double *t)
+{
+	if (!h || !t)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "get_time: bad arguments");
+	*t = h->t;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_state_size(gdn_cuda_handle *h, long long *wlen)
+{
+	if (!h || !wlen)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "state_size: bad arguments");
+	*wlen = (h->scheme == GDN_CUDA_SCHEME_RK3 ? 6LL : 6LL * h->nv) * h->neq;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_num_levels(gdn_cuda_handle *h, int *nlevels)
+{
+	if (!h || !nlevels)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "num_levels: bad arguments");
+	*nlevels = h->scheme == GDN_CUDA_SCHEME_KINETIC ? (int)h->level_off.size() - 1 : 0;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_launch_count(gdn_cuda_handle *h, long long *count)
+{
+	if (!h || !count)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "launch_count: bad arguments");
+	*count = h->launches;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_stream(gdn_cuda_handle *h, void **stream)
+{
+	if (!h || !stream)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "stream: bad arguments");
+	*stream = (void *)h->stream;
+	return GDN_CUDA_OK;
+}

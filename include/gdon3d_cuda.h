@@ -1,0 +1,199 @@
+/*
+ * gdon3d_cuda.h -- C-ABI of the B200 (sm_100a) implementation of Gdon3d's two
+ * data-parallel hot paths:
+ *   HP-1  the P2-tetrahedron DG residual driven by the low-storage RK3
+ *         (reference: src/dg/explicit.c:39-117, src/simulation/simulation.c
+ *          :218-491, src/models/maxwell.c:152-192, src/dg/dg.c:61-107);
+ *   HP-2  the CFL-less kinetic-relaxation step: per-velocity Crank-Nicolson
+ *         DG transport solves and the relaxation to the Maxwell equilibrium
+ *         (reference: src/dg/relaxation.c:24-185, src/simulation/simulation.c
+ *          :493-604, src/models/d3q4.c:82-301, src/dg/dg.c:109-147).
+ *
+ * Plain C types only (ints, doubles, pointers, sizes).  Every call returns an
+ * int status (GDN_CUDA_OK = 0) and never aborts; gdn_cuda_last_error() gives
+ * the message of the last failure on the calling thread.
+ *
+ * State vectors passed across this boundary use the reference's layout for
+ * gdn_simulation.wn (src/simulation/simulation.h:17-38):
+ *   RK3     wn[(ipg) * 6 + iw]            (simulation.c:211-214)
+ *   kinetic wn[(iw * nb_v + iv) * neq + ipg]   (simulation.c:22-54)
+ * with ipg in [0, neq), neq = 10 * nbelems + 6 * nboundaryfaces: the volume
+ * nodes 10 * ie + iloc first, then the boundary dofs 6 * ibf + iloc.
+ */
+#ifndef GDON3D_CUDA_H
+#define GDON3D_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GDN_CUDA_OK 0
+#define GDN_CUDA_ERR_CUDA 1 /* a CUDA runtime call failed */
+#define GDN_CUDA_ERR_INVALID 2 /* bad argument, size or descriptor */
+#define GDN_CUDA_ERR_UNSUPPORTED 3 /* model/physics not available on device */
+#define GDN_CUDA_ERR_CYCLE 4 /* the upwind element graph has a cycle */
+#define GDN_CUDA_ERR_OOM 5 /* device allocation failed */
+#define GDN_CUDA_ERR_TIMEOUT 6 /* a bounded device-side wait gave up */
+#define GDN_CUDA_ERR_MESH 7 /* inconsistent mesh (bad index, det <= 0) */
+
+/* ---- inputs ------------------------------------------------------------ */
+
+/* The arrays of the reference's gdn_mesh after mesh_build_connectivity
+ * (src/mesh/mesh.h:15-45, built at src/mesh/mesh.c:1234-1268). */
+typedef struct gdn_cuda_mesh {
+	int nbelems;
+	int nbfaces;
+	int nboundaryfaces;
+	int nbqnodes; /* nbqnodes_in */
+	const int *face2elem; /* [4*nbfaces] eL, locfaceL, eR (-1), locfaceR (-1) */
+	const int *fnode2enode; /* [12*nbfaces] L then R local node ids */
+	const int *boundaryface; /* [nboundaryfaces] global face ids */
+	const int *elem2qnode; /* [10*nbelems + 6*nboundaryfaces] */
+	const double *node; /* [3*nbqnodes] P2 node coordinates */
+} gdn_cuda_mesh;
+
+/* The reference's P2 tables, as returned by its accessors
+ * t10_get_wpg_ref_entry, t10_get_inv_mass_ref_entry,
+ * t10_get_internal_ref_entry, t10_get_face_scale_entry,
+ * t10_get_ref_normal_entry, t10_get_ref_face2node_entry
+ * (src/mesh/t10.h:72-86).  gdn_cuda_t10_tables() fills the same values. */
+typedef struct gdn_cuda_tables {
+	double wpg[10];
+	double mass[10][10];
+	double inv_mass[10][10];
+	double internal[10][10][3]; /* [i][j][k] = int d_k(phi_i) phi_j */
+	double face_scal[6][6];
+	double ref_normal[4][3];
+	int face2node[4][6];
+} gdn_cuda_tables;
+
+/* Analytic data evaluated on the device (boundary values, initial data and
+ * the error norm).  The reference passes a host callback
+ * (gdn_model.get_imposed_data, src/models/model.h:24-25); the GPU path needs
+ * a descriptor instead.  PLANE: E = amp pol sin(kmag (khat.x - t) + phase),
+ * H = khat x E.  CAVITY: maxwell_imposed_macro_cavity
+ * (src/models/maxwell.c:118-133) with its constants. */
+#define GDN_CUDA_DATA_PLANE 0
+#define GDN_CUDA_DATA_CAVITY 1
+typedef struct gdn_cuda_data {
+	int kind;
+	double khat[3];
+	double kmag;
+	double pol[3];
+	double amp;
+	double phase;
+} gdn_cuda_data;
+
+/* The recognised gdn_model (src/models/model.h:41-62): Maxwell with the
+ * upwind flux maxwell_num_flux_upwind (also as the boundary flux), either
+ * through RK3 (use_relax_scheme = false) or through the CFL-less scheme with
+ * the d3q4 (nb_v = 4, d3q4.c:17-42) or d3q6 (nb_v = 6, d3q6.c:18-47)
+ * velocity set. */
+#define GDN_CUDA_SCHEME_RK3 0
+#define GDN_CUDA_SCHEME_KINETIC 1
+typedef struct gdn_cuda_model {
+	int scheme;
+	int nb_w; /* must be 6 */
+	int nb_v; /* 4 or 6 for the kinetic scheme, ignored for RK3 */
+	double lambda; /* model->lambda */
+	double omega; /* model->omega (relaxation) */
+	const double *vi; /* [3*nb_v] model->vi */
+	double theta; /* 0.5 in the reference (relaxation.c:133) */
+} gdn_cuda_model;
+
+#define GDN_CUDA_FP64 0 /* FP64 storage and arithmetic */
+#define GDN_CUDA_FP32 1 /* FP32 storage and arithmetic, FP64 setup and norms */
+#define GDN_CUDA_FP32_REFINE 2 /* kinetic: FP64 state, FP32 sweeps, FP64 residual refinement */
+#define GDN_CUDA_BF16_STORE 3 /* kinetic: BF16 distributions, FP32 arithmetic */
+typedef struct gdn_cuda_config {
+	int precision;
+	int refine_passes; /* GDN_CUDA_FP32_REFINE: FP64-residual passes (1 or 2) */
+	int elems_per_cta; /* RK3 element tile; 0 = autotuned */
+	int use_graph; /* capture step loops as CUDA graphs (1 = yes) */
+	int device; /* CUDA device ordinal */
+} gdn_cuda_config;
+
+typedef struct gdn_cuda_handle gdn_cuda_handle;
+
+/* ---- setup ------------------------------------------------------------- */
+
+/* Fills `t` with the P2 tables computed from the P2 basis (exact rational
+ * integrals; the face mass is rounded to 10 significant digits as the
+ * reference's t10_face_scal, src/mesh/t10.c:1317-1330). */
+int gdn_cuda_t10_tables(gdn_cuda_tables *t);
+
+/* Builds the reference's connectivity arrays (the outputs of
+ * mesh_build_connectivity, src/mesh/mesh.c:1234-1268) from T4 vertices:
+ * coords[3*nbnodes], elem2node[4*nbelems] (0-based, positively oriented).
+ * First call with NULL outputs to get the sizes (nbfaces, nboundaryfaces,
+ * nbqnodes), then with arrays of those sizes:
+ * face2elem[4*nbfaces], fnode2enode[12*nbfaces], boundaryface[nbf],
+ * elem2qnode[10*nbelems + 6*nbf], node[3*nbqnodes]. */
+int gdn_cuda_mesh_build(int nbnodes, const double *coords, int nbelems,
+						const int *elem2node, int *nbfaces,
+						int *nboundaryfaces, int *nbqnodes, int *face2elem,
+						int *fnode2enode, int *boundaryface, int *elem2qnode,
+						double *node);
+
+/* h_min = min over elements of volume / surface (mesh_get_t4_hmin,
+ * src/mesh/mesh.c:149-210). */
+int gdn_cuda_mesh_hmin(const gdn_cuda_mesh *mesh, double *hmin);
+
+/* Replaces the operator assembly of dg_solve_rk3 (assemble_rk3,
+ * src/dg/explicit.c:25-37) and dg_solve_relaxation (assemble_theta_scheme,
+ * src/dg/relaxation.c:24-91): uploads the mesh, derives geometry on the
+ * device (FP64), builds the upwind level schedules and block inverses for
+ * the kinetic scheme at this dt.  dt is simu->dt. */
+int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
+					const gdn_cuda_model *model, const gdn_cuda_data *data,
+					const gdn_cuda_config *config, double dt,
+					gdn_cuda_handle **out);
+
+int gdn_cuda_detach(gdn_cuda_handle *h);
+
+/* ---- the path ---------------------------------------------------------- */
+
+/* Replaces dg_solve (src/dg/dg.c:23-30): dg_init_sol_macro on the device,
+ * itermax time steps, then the final state is written to wn (reference
+ * layout, m * neq doubles, boundary dofs included), *t to the final time and
+ * *cpu_running_t to the wall time of the time loop (seconds, as
+ * simu->cpu_running_t). */
+int gdn_cuda_solve(gdn_cuda_handle *h, int itermax, double *wn, double *t,
+				   double *cpu_running_t);
+
+/* dg_init_sol_macro (src/dg/dg.c:32-59) on the device; sets t = 0. */
+int gdn_cuda_init(gdn_cuda_handle *h);
+
+/* Device-resident time steps (no host copies). */
+int gdn_cuda_advance(gdn_cuda_handle *h, int nsteps);
+
+/* Host state in / out, reference layout; t is the time the state is at. */
+int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t);
+int gdn_cuda_get_state(gdn_cuda_handle *h, double *wn);
+
+/* One call a caller makes per chunk of a run: copies wn (host, reference
+ * layout) to the device, advances nsteps, copies the result back into wn. */
+int gdn_cuda_step_host(gdn_cuda_handle *h, double *wn, int nsteps);
+
+/* simulation_error_l2 (src/simulation/simulation.c:606-666) of the device
+ * state at the current time: mean over the 6 fields of the nodal-quadrature
+ * L2 norm of (w - w_exact).  FP64, deterministic. */
+int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err);
+
+/* ---- introspection ------------------------------------------------------ */
+int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
+/* wlen = m * neq of the reference layout */
+int gdn_cuda_state_size(gdn_cuda_handle *h, long long *wlen);
+/* kinetic: number of sweep levels of the schedule (0 for RK3) */
+int gdn_cuda_num_levels(gdn_cuda_handle *h, int *nlevels);
+/* kernels launched by this handle since attach (for launch accounting) */
+int gdn_cuda_launch_count(gdn_cuda_handle *h, long long *count);
+/* the CUDA stream the handle launches on (a cudaStream_t) */
+int gdn_cuda_stream(gdn_cuda_handle *h, void **stream);
+const char *gdn_cuda_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

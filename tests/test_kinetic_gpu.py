@@ -1,0 +1,61 @@
+"""HP-2 parity on the GPU: the CFL-less kinetic step (level-scheduled block
+sweeps + relaxation) against the reference's dg_solve_relaxation compiled from
+its own sources (the sparse LU is the repo's exact direct-solve shim; parity
+against KLU itself is unpinned because KLU is not installed)."""
+import numpy as np
+import pytest
+
+from gdon3d_b200 import capi, kuhn
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(n, jitter, steps, cfl_mult, nb_v=4, data="cavity", precision=capi.FP64, seed=5):
+    c, e = kuhn.kuhn_cube(n, jitter, seed=seed)
+    mesh = capi.mesh_build(c, e)
+    dt = cfl_mult * 0.3 * mesh.hmin()
+    if data == "cavity":
+        gd, rd = capi.cavity_data(), ref.make_data(kind=ref.DATA_CAVITY)
+    else:
+        kw = dict(khat=(1, 0, 0), kmag=2 * np.pi, pol=(0, 1, 0))
+        gd, rd = capi.plane_data(**kw), ref.make_data(**kw)
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, gd, dt, nb_v=nb_v, precision=precision)
+    wn, t, _ = s.solve(steps)
+    err = s.error_l2()
+    levels = s.num_levels
+    s.close()
+    r = ref.RefMesh(c, e).run(ref.SCHEME_D3Q4 if nb_v == 4 else ref.SCHEME_D3Q6, rd, dt, steps)
+    return wn, t, err, r, levels
+
+
+@pytest.mark.parametrize("n,jitter,steps,mult", [(2, 0.0, 5, 10), (4, 0.15, 10, 10), (4, 0.0, 10, 20)])
+def test_kinetic_d3q4_fp64_matches_reference(n, jitter, steps, mult):
+    wn, t, err, r, levels = _pair(n, jitter, steps, mult)
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= 1e-12, rel
+    assert t == r["t"]
+    assert abs(err - r["err"]) <= 1e-10 * r["err"]
+    assert levels >= 1
+
+
+def test_kinetic_d3q6_plane_fp64_matches_reference():
+    wn, t, err, r, _ = _pair(3, 0.1, 6, 10, nb_v=6, data="plane")
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= 1e-12, rel
+
+
+def test_kinetic_cfg2_cavity_16_fp64_matches_reference():
+    """16^3 x 6 tets, cavity, dt = 10 x the RK3 CFL
+    step, 100 steps, d3q4."""
+    wn, t, err, r, levels = _pair(16, 0.0, 100, 10)
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= 1e-12, rel
+    assert abs(err - r["err"]) <= 1e-10 * r["err"]
+
+
+def test_kinetic_fp32_close_to_reference():
+    wn, t, err, r, _ = _pair(8, 0.0, 20, 10, precision=capi.FP32)
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= 1e-4, rel
+    assert abs(err - r["err"]) <= 0.01 * r["err"]
