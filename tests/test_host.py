@@ -1,0 +1,138 @@
+"""CPU: the C-ABI library loads and exports every symbol of
+include/gdon3d_cuda.h; host-side logic (P2 tables, connectivity builder,
+hmin, argument validation, mesh generator) against the reference's golden
+fixtures.  No GPU compute is called here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from gdon3d_b200 import capi, kuhn
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _golden(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def test_library_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "gdon3d_cuda.h")).read()
+    declared = set(re.findall(r"\b(gdn_cuda_[a-z0-9_]+)\s*\(", hdr))
+    assert declared, "no declarations found"
+    L = capi.lib()
+    for name in sorted(declared):
+        assert hasattr(L, name), name
+    assert declared == set(capi.EXPORTS)
+
+
+def test_tables_match_reference_tables():
+    g = _golden("kuhn2")
+    t = capi.tables_as_numpy(capi.t10_tables())
+    # face mass: the reference's 10-digit literals, bit for bit
+    assert np.array_equal(t["face_scal"], g["t10_face_scal"])
+    assert np.array_equal(t["face2node"], g["t10_face2node"])
+    assert np.array_equal(t["mass"], g["t10_mass"])
+    assert np.array_equal(t["inv_mass"], g["t10_inv_mass"])
+    # exact rationals vs the reference's decimal literals: within 1 ulp (two
+    # wpg entries, 1/sqrt(3) in the face-3 normal, 1e-18 noise in internal)
+    for k in ("wpg", "internal", "ref_normal"):
+        assert np.max(np.abs(t[k] - g["t10_" + k])) <= 2.3e-16, k
+
+
+@pytest.mark.parametrize("name", ["kuhn2", "kuhn3j"])
+def test_mesh_build_matches_reference_connectivity(name):
+    g = _golden(name)
+    m = capi.mesh_build(g["coords"], g["elem2node"])
+    assert np.array_equal(m.face2elem, g["mesh_face2elem"])
+    assert np.array_equal(m.fnode2enode, g["mesh_fnode2enode"])
+    assert np.array_equal(m.boundaryface, g["mesh_boundaryface"])
+    # P2 node ids are numbered differently; the coordinates of every
+    # (element, local node) and boundary dof must be identical bit for bit
+    x_ours = m.node.reshape(-1, 3)[m.elem2qnode]
+    x_ref = g["mesh_node"].reshape(-1, 3)[g["mesh_elem2qnode"]]
+    assert np.array_equal(x_ours, x_ref)
+    assert m.hmin() == float(g["hmin"])
+
+
+def test_mesh_build_rejects_bad_indices():
+    c, e = kuhn.kuhn_cube(1)
+    e = e.copy()
+    e[0, 0] = 999
+    with pytest.raises(capi.GdnError) as ex:
+        capi.mesh_build(c, e)
+    assert ex.value.code == capi.ERR_MESH
+
+
+def test_attach_validates_before_touching_the_device():
+    c, e = kuhn.kuhn_cube(2)
+    m = capi.mesh_build(c, e)
+    bad = capi.plane_data(khat=(1, 1, 0), pol=(0, 0, 1))  # not a unit vector
+    with pytest.raises(capi.GdnError) as ex:
+        capi.Solver(m, capi.SCHEME_RK3, bad, 0.01)
+    assert ex.value.code == capi.ERR_INVALID
+    with pytest.raises(capi.GdnError) as ex:
+        capi.Solver(m, capi.SCHEME_RK3, capi.plane_data(), -1.0)
+    assert ex.value.code == capi.ERR_INVALID
+    with pytest.raises(capi.GdnError) as ex:
+        capi.Solver(m, capi.SCHEME_KINETIC, capi.cavity_data(), 0.01, nb_v=5)
+    assert ex.value.code == capi.ERR_UNSUPPORTED
+    # corrupt connectivity: an element index out of range
+    f2e = m.face2elem.copy()
+    f2e[0] = 10 ** 6
+    m2 = capi.MeshArrays(f2e, m.fnode2enode, m.boundaryface, m.elem2qnode, m.node, m.nbelems)
+    with pytest.raises(capi.GdnError) as ex:
+        capi.Solver(m2, capi.SCHEME_RK3, capi.plane_data(), 0.01)
+    assert ex.value.code == capi.ERR_MESH
+    assert "face2elem" in str(ex.value)
+
+
+def test_null_handle_calls_fail_cleanly():
+    L = capi.lib()
+    assert L.gdn_cuda_advance(None, 1) == capi.ERR_INVALID
+    assert L.gdn_cuda_detach(None) == capi.ERR_INVALID
+    d = C.c_double()
+    assert L.gdn_cuda_error_l2(None, C.byref(d)) == capi.ERR_INVALID
+    assert b"bad arguments" in L.gdn_cuda_last_error()
+
+
+@pytest.mark.parametrize("n,jitter", [(1, 0.0), (3, 0.0), (4, 0.15), (6, 0.3)])
+def test_kuhn_mesh_is_conforming_and_positive(n, jitter):
+    c, e = kuhn.kuhn_cube(n, jitter, seed=5)
+    assert len(e) == 6 * n ** 3 and len(c) == (n + 1) ** 3
+    p = c[e]
+    det = np.einsum("ij,ij->i", p[:, 1] - p[:, 0], np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]))
+    assert (det > 0).all()
+    assert abs(det.sum() / 6.0 - 1.0) < 1e-12  # volumes tile the unit cube
+    m = capi.mesh_build(c, e)
+    assert m.nboundaryfaces == 12 * n * n
+    assert m.nbfaces == (4 * len(e) + m.nboundaryfaces) // 2
+    # boundary vertices never move
+    on_b = (np.abs(c) < 1e-15) | (np.abs(c - 1) < 1e-15)
+    assert on_b.any(axis=1).sum() == (n + 1) ** 3 - max(n - 1, 0) ** 3
+
+
+def test_kuhn_jitter_is_seeded():
+    a, _ = kuhn.kuhn_cube(4, 0.15, seed=9)
+    b, _ = kuhn.kuhn_cube(4, 0.15, seed=9)
+    c, _ = kuhn.kuhn_cube(4, 0.15, seed=10)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    base, _ = kuhn.kuhn_cube(4, 0.0)
+    assert np.max(np.abs(a - base)) <= 0.15 / 4 + 1e-15
+
+
+def test_msh22_roundtrip(tmp_path):
+    c, e = kuhn.kuhn_cube(2, 0.1, seed=2)
+    p = str(tmp_path / "m.msh")
+    kuhn.write_msh22(p, c, e)
+    c2, e2 = kuhn.read_msh22(p)
+    assert np.array_equal(c, c2) and np.array_equal(e, e2)
+
+
+def test_random_plane_wave_is_orthonormal():
+    k, kmag, p = kuhn.random_plane_wave(3, 4 * np.pi)
+    assert abs(np.linalg.norm(k) - 1) < 1e-15 and abs(np.linalg.norm(p) - 1) < 1e-15
+    assert abs(np.dot(k, p)) < 1e-15 and kmag == 4 * np.pi

@@ -59,3 +59,28 @@ def test_kinetic_fp32_close_to_reference():
     rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
     assert rel <= 1e-4, rel
     assert abs(err - r["err"]) <= 0.01 * r["err"]
+
+
+import os  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("name,nb_v", [("kuhn2", 4), ("kuhn3j", 4), ("kuhn2", 6)])
+def test_kinetic_fp64_matches_golden_fixture(name, nb_v):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    arrays = {k[5:]: g[k] for k in g.files if k.startswith("mesh_")}
+    mesh = capi.MeshArrays(arrays["face2elem"], arrays["fnode2enode"], arrays["boundaryface"],
+                           arrays["elem2qnode"], arrays["node"], int(g["nbelems"]))
+    tabs = capi.tables_from_numpy({k[4:]: g[k] for k in g.files if k.startswith("t10_")})
+    if nb_v == 4:
+        data, key = capi.cavity_data(), "q4"
+    else:
+        p = g["plane"]
+        data, key = capi.plane_data(khat=p[:3], kmag=p[3], pol=p[4:7]), "q6"
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, data, 10 * float(g["dt"]), nb_v=nb_v, tables=tabs)
+    wn, t, _ = s.solve(int(g[key + "_steps"]))
+    s.close()
+    rel = np.linalg.norm(wn - g[key + "_wn"]) / np.linalg.norm(g[key + "_wn"])
+    assert rel <= 1e-12, rel
+    assert t == float(g[key + "_t"])

@@ -57,3 +57,68 @@ def test_rk3_fp32_close_to_reference():
     # discretisation error (~5e-4 relative to the field at this size)
     assert rel <= 2e-5, rel
     assert abs(err - r["err"]) <= 0.01 * r["err"]
+
+
+import os  # noqa: E402
+
+from oracle import port  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("name", ["kuhn2", "kuhn3j"])
+def test_rk3_fp64_matches_golden_fixture(name):
+    """Against the committed vectors of the reference's own dg_solve_rk3
+    (tests/golden/make_golden.py), with the reference's tables passed through
+    the C-ABI as a reference host would."""
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    arrays = {k[5:]: g[k] for k in g.files if k.startswith("mesh_")}
+    mesh = capi.MeshArrays(arrays["face2elem"], arrays["fnode2enode"], arrays["boundaryface"],
+                           arrays["elem2qnode"], arrays["node"], int(g["nbelems"]))
+    tabs = capi.tables_from_numpy({k[4:]: g[k] for k in g.files if k.startswith("t10_")})
+    p = g["plane"]
+    s = capi.Solver(mesh, capi.SCHEME_RK3, capi.plane_data(khat=p[:3], kmag=p[3], pol=p[4:7]),
+                    float(g["dt"]), tables=tabs)
+    wn, t, _ = s.solve(int(g["rk3_steps"]))
+    err = s.error_l2()
+    s.close()
+    rel = np.linalg.norm(wn - g["rk3_wn"]) / np.linalg.norm(g["rk3_wn"])
+    assert rel <= FP64_RTOL, rel
+    assert t == float(g["rk3_t"])
+    assert abs(err - float(g["rk3_err"])) <= 1e-10 * float(g["rk3_err"])
+
+
+def test_rk3_fp64_matches_oracle_16():
+    c, e = kuhn.kuhn_cube(16, 0.15, seed=21)
+    mesh = capi.mesh_build(c, e)
+    dt = 0.3 * mesh.hmin()
+    kw = dict(khat=(0.0, 0.6, 0.8), kmag=4 * np.pi, pol=(1.0, 0.0, 0.0))
+    s = capi.Solver(mesh, capi.SCHEME_RK3, capi.plane_data(**kw), dt)
+    wn, t, _ = s.solve(12)
+    s.close()
+    arrays = dict(face2elem=mesh.face2elem, fnode2enode=mesh.fnode2enode,
+                  boundaryface=mesh.boundaryface, elem2qnode=mesh.elem2qnode, node=mesh.node)
+    o = port.Oracle(mesh.nbelems, arrays, capi.tables_as_numpy(capi.t10_tables()))
+    wo, to = o.rk3(port.Oracle.data(**kw), dt, 12)
+    rel = np.linalg.norm(wn - wo) / np.linalg.norm(wo)
+    assert rel <= FP64_RTOL, rel
+    assert t == to
+
+
+def test_rk3_step_host_equals_device_resident_steps():
+    """gdn_cuda_step_host (host state in/out) gives the same state as
+    advancing on the device."""
+    c, e = kuhn.kuhn_cube(4, 0.1, seed=2)
+    mesh = capi.mesh_build(c, e)
+    dt = 0.3 * mesh.hmin()
+    s = capi.Solver(mesh, capi.SCHEME_RK3, capi.plane_data(), dt)
+    s.init()
+    s.advance(3)
+    w3 = s.get_state()
+    s.advance(4)
+    w7 = s.get_state()
+    host = w3.copy()
+    s.set_state(host, 3 * dt)
+    s.step_host(host, 4)
+    s.close()
+    assert np.array_equal(host[: 60 * mesh.nbelems], w7[: 60 * mesh.nbelems])
