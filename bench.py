@@ -182,6 +182,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_CUBE, help="cube resolution (default 96)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", default="both", choices=["both", "fp64", "fp32"],
+                    help="profiling aid: run one precision variant only")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -224,6 +227,8 @@ def main():
     results = {}
     states = {}
     for name, prec, b_s in (("fp64", capi.FP64, 8), ("fp32", capi.FP32, 4)):
+        if args.only not in ("both", name):
+            continue
         s = capi.Solver(mesh, capi.SCHEME_RK3, data, dt, precision=prec, device=local)
         st = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
         s.init()
@@ -254,25 +259,33 @@ def main():
                          "algorithmic_bytes_per_launch": alg / 3,
                          "traffic": dram_traffic("rk3_stage_%s_n%d" % (name, n))},
             "solver": s}
-    ref64 = states["fp64"][: 60 * ne]
-    rel_fp32 = float(np.linalg.norm(states["fp32"][: 60 * ne] - ref64) / np.linalg.norm(ref64))
+    rel_fp32 = None
+    if "fp64" in states and "fp32" in states:
+        ref64 = states["fp64"][: 60 * ne]
+        rel_fp32 = float(np.linalg.norm(states["fp32"][: 60 * ne] - ref64) / np.linalg.norm(ref64))
+    head = results["fp32"] if "fp32" in results else results["fp64"]
 
     # e2e through the C-ABI with host buffers: one gdn_cuda_step_host call of K
     # steps (H2D of the reference-layout state from pinned memory, K steps, D2H)
-    s32 = results["fp32"]["solver"]
-    wl = s32.wlen
-    host = torch.empty(wl, dtype=torch.float64, pin_memory=True)
-    hv = host.numpy()
-    hv[:] = states["fp32"]
-    s32.step_host(hv, 1)  # warm the host path
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    s32.step_host(hv, K)
-    t1 = time.perf_counter()
-    barrier()
-    e2e_s = max_over_ranks(t1 - t0)
-    state_bytes = wl * 8
+    e2e = None
+    if not args.no_e2e:
+        sh = head["solver"]
+        wl = sh.wlen
+        host = torch.empty(wl, dtype=torch.float64, pin_memory=True)
+        hv = host.numpy()
+        hv[:] = states["fp32" if "fp32" in states else "fp64"]
+        sh.step_host(hv, 1)  # warm the host path
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sh.step_host(hv, K)
+        t1 = time.perf_counter()
+        barrier()
+        e2e_s = max_over_ranks(t1 - t0)
+        e2e = {"value": world * dofs_per_step * K / e2e_s, "unit": "DoF-updates/s",
+               "h2d_bytes_per_step": wl * 8 / K, "d2h_bytes_per_step": wl * 8 / K,
+               "call": "gdn_cuda_step_host: reference-layout FP64 state in pinned host memory, "
+                       "copied in, %d steps, copied out" % K}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -284,28 +297,27 @@ def main():
 
     for r in results.values():
         r.pop("solver").close()
-    f32 = results["fp32"]
     line = {
-        "metric": "DoF-updates/s", "value": f32["value"], "unit": "DoF-updates/s", "n_gpus": world,
-        "steps": K, "warmup": W, "ms_per_step": f32["ms_per_step"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_elements": ne, "p": 2, "fields": 6, "steps_timed": K,
+        "metric": "DoF-updates/s", "value": head["value"], "unit": "DoF-updates/s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if "fp32" in results else "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD if n == N_CUBE else WORKLOAD.replace("96", str(n)),
+                   "n_elements": ne, "p": 2, "fields": 6, "steps_timed": K,
                    "dt": dt, "cfl": CFL, "seed": SEED, "khat": list(map(float, khat)), "kmag": kmag,
                    "precision": "FP32 state and residual arithmetic; FP64 geometry setup and norms",
                    "l2_flush": "inputs larger than L2: FP32 state %.2f GB per buffer vs 126 MB L2"
                                % (60 * ne * 4 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single-gpu"},
-        "roofline": f32["roofline"], "clocks": f32["clocks"], "gpu_launches": f32["gpu_launches"],
+        "roofline": head["roofline"], "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
         "l2_rel_fp32_vs_fp64": rel_fp32,
-        "l2_error_vs_analytic": {"fp32": f32["l2_error_vs_analytic"],
-                                 "fp64": results["fp64"]["l2_error_vs_analytic"]},
-        "variants": {"fp64_plain": {k: results["fp64"][k] for k in
-                                    ("value", "ms_per_step", "roofline", "clocks", "gpu_launches")}},
-        "speedup_fp32_vs_fp64": f32["value"] / results["fp64"]["value"],
-        "e2e": {"value": world * dofs_per_step * K / e2e_s, "unit": "DoF-updates/s",
-                "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K,
-                "call": "gdn_cuda_step_host: reference-layout FP64 state in pinned host memory, "
-                        "copied in, %d steps, copied out" % K},
+        "l2_error_vs_analytic": {k: v["l2_error_vs_analytic"] for k, v in results.items()},
+        "variants": {k + ("_plain" if k == "fp64" else ""):
+                     {q: v[q] for q in ("value", "ms_per_step", "roofline", "clocks", "gpu_launches")}
+                     for k, v in results.items()},
+        "speedup_fp32_vs_fp64": (results["fp32"]["value"] / results["fp64"]["value"]
+                                 if len(results) == 2 else None),
+        "e2e": e2e,
         "cpu_baseline": cpu,
     }
     if rank == 0:

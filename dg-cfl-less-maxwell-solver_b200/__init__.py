@@ -8,3 +8,5 @@ This directory is loaded as the Python package `gdon3d_b200` (its on-disk
 name is not a Python identifier): see load_package() in tests/conftest.py and
 bench.py.
 """
+
+from . import capi, kuhn  # noqa: E402,F401

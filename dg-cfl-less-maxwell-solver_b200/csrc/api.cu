@@ -69,6 +69,7 @@ struct gdn_cuda_handle {
 	long long steps = 0;
 	long long launches = 0;
 	int ssize = 8; // bytes per stored state value
+	int rk3_sparse = 1; // tables follow the P2 structural-zero pattern
 	// device arrays
 	std::vector<DevBuf> bufs;
 	int *e2q = nullptr;
@@ -150,6 +151,7 @@ static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
 	for (int i = 0; i < 6; i++)
 		for (int j = 0; j < 6; j++)
 			o.S[i][j] = (T)t->face_scal[i][j];
+	o.n3scale = (T)(t->ref_normal[3][0] * std::sqrt(3.0));
 	for (int f = 0; f < 4; f++) {
 		for (int k = 0; k < 3; k++)
 			o.ref_normal[f][k] = t->ref_normal[f][k];
@@ -363,6 +365,9 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 	const long long ne = h->ne, nf = h->nf, nbf = h->nbf;
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
 	GDN_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+	if (!rk3_tables_standard_faces(t))
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: face2node differs from the P2 convention");
+	h->rk3_sparse = rk3_tables_sparse(t) ? 1 : 0;
 	GDN_TRY(upload_tables(t));
 	std::vector<int> nb, perm;
 	std::vector<double> bx;
@@ -582,6 +587,7 @@ static int rk3_step(gdn_cuda_handle *h)
 		p.B = RK_B[i];
 		p.stage0 = i == 0;
 		p.write_k2 = i < 2;
+		p.sparse = h->rk3_sparse;
 		GDN_TRY(launch_rk3_stage<T>(p, h->stream));
 		h->launches++;
 		h->cur = 1 - h->cur;

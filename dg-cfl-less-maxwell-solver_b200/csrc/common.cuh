@@ -24,6 +24,7 @@ struct Tables {
 	T S[NQV][NQV];
 	T wpg[NQN];
 	double ref_normal[4][3];
+	T n3scale; // ref_normal[3][k] * sqrt(3): the face-3 scale of the reference
 	int f2n[4][NQV];
 	// node -> (face, position on the face) list; vertex nodes lie on 3
 	// faces, edge nodes on 2
@@ -86,6 +87,18 @@ __device__ __forceinline__ void exact_w(const Data &d, const double x[3], double
 	}
 }
 
+// 1 / (sqrt(nn) + 1e-16) as in maxwell_num_flux_upwind; in FP32 the 1e-16
+// is far below the rounding of |n| and the hardware reciprocal square root
+// is used.
+__device__ __forceinline__ double inv_norm_eps(double nn)
+{
+	return 1.0 / (sqrt(nn) + 1e-16);
+}
+__device__ __forceinline__ float inv_norm_eps(float nn)
+{
+	return rsqrtf(nn);
+}
+
 // Upwind Maxwell flux (maxwell_num_flux_upwind, src/models/maxwell.c:152-192):
 // with {w} = (wR + wL)/2, [w] = (wR - wL)/2 and r = 1/(|n| + 1e-16),
 //   F_E = -n x {H} + r n x (n x [E]),   F_H = n x {E} + r n x (n x [H]).
@@ -93,7 +106,7 @@ template <typename T>
 __device__ __forceinline__ void upwind_flux(const T wL[6], const T wR[6], const T n[3], T F[6])
 {
 	const T nn = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
-	const T r = T(1) / (sqrt(nn) + T(1e-16));
+	const T r = inv_norm_eps(nn);
 	T Es[3], Hs[3], Ed[3], Hd[3];
 #pragma unroll
 	for (int c = 0; c < 3; c++) {

@@ -19,7 +19,11 @@ struct Rk3Params {
 	double t_stage, dt, A, B;
 	int stage0; // k2 = -dt dw (no k2 read)
 	int write_k2; // 0 on the last stage: k2 is dead until the next stage 0
+	int sparse; // tables follow the P2 structural-zero pattern
 };
+
+bool rk3_tables_sparse(const gdn_cuda_tables *t);
+bool rk3_tables_standard_faces(const gdn_cuda_tables *t);
 
 template <typename T>
 int launch_rk3_stage(const Rk3Params<T> &p, cudaStream_t s);

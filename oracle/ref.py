@@ -38,6 +38,26 @@ def make_data(kind=DATA_PLANE, khat=(1.0, 0.0, 0.0), kmag=2 * np.pi,
 
 
 _libs: dict = {}
+_libc = C.CDLL(None)
+
+
+class _stdout_to_stderr:
+    """The reference prints progress to stdout (explicit.c:98-101,
+    relaxation.c:167-170); keep the caller's stdout clean by sending C stdout
+    to stderr while reference code runs."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        _libc.fflush(None)
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        _libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
 
 
 def available(variant: str = "zero") -> bool:
@@ -86,7 +106,8 @@ class RefMesh:
     def __init__(self, coords=None, elem2node=None, path=None, variant="zero"):
         self.L = lib(variant)
         if path is not None:
-            self.h = self.L.ref_mesh_from_file(path.encode())
+            with _stdout_to_stderr():
+                self.h = self.L.ref_mesh_from_file(path.encode())
         else:
             c = np.ascontiguousarray(coords, dtype=np.float64)
             e = np.ascontiguousarray(elem2node, dtype=np.int32)
@@ -117,8 +138,9 @@ class RefMesh:
         wlen = self.L.ref_wlen(self.h, scheme)
         wn = np.zeros(wlen, np.float64)
         t, err, crun, casm = (C.c_double() for _ in range(4))
-        rc = self.L.ref_run(self.h, scheme, C.byref(data), dt, steps, _dp(wn),
-                            C.byref(t), C.byref(err), C.byref(crun), C.byref(casm))
+        with _stdout_to_stderr():
+            rc = self.L.ref_run(self.h, scheme, C.byref(data), dt, steps, _dp(wn),
+                                C.byref(t), C.byref(err), C.byref(crun), C.byref(casm))
         if rc != 0:
             raise RuntimeError("reference run did not produce %d steps" % steps)
         return dict(wn=wn, t=t.value, err=err.value, cpu_run=crun.value,

@@ -115,10 +115,11 @@ def test_rk3_step_host_equals_device_resident_steps():
     s.init()
     s.advance(3)
     w3 = s.get_state()
+    t3 = s.t
     s.advance(4)
     w7 = s.get_state()
     host = w3.copy()
-    s.set_state(host, 3 * dt)
+    s.set_state(host, t3)
     s.step_host(host, 4)
     s.close()
     assert np.array_equal(host[: 60 * mesh.nbelems], w7[: 60 * mesh.nbelems])
