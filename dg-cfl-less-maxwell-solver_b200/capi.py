@@ -69,7 +69,7 @@ EXPORTS = [
     "gdn_cuda_detach", "gdn_cuda_solve", "gdn_cuda_init", "gdn_cuda_advance",
     "gdn_cuda_set_state", "gdn_cuda_get_state", "gdn_cuda_step_host", "gdn_cuda_error_l2",
     "gdn_cuda_get_time", "gdn_cuda_state_size", "gdn_cuda_num_levels", "gdn_cuda_launch_count",
-    "gdn_cuda_stream", "gdn_cuda_last_error",
+    "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc",
 ]
 
 _lib = None
@@ -102,6 +102,8 @@ def lib():
     L.gdn_cuda_num_levels.argtypes = [vp, ip]
     L.gdn_cuda_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.gdn_cuda_stream.argtypes = [vp, C.POINTER(vp)]
+    L.gdn_cuda_error_l2_noalloc.argtypes = [vp, vp, vp, C.c_longlong, dp, C.POINTER(Data),
+                                            C.c_double, vp, dp]
     _lib = L
     return L
 

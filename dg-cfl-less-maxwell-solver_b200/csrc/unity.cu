@@ -5,3 +5,4 @@
 #include "rk3.cu"
 #include "kinetic.cu"
 #include "api.cu"
+#include "noalloc.cu"

@@ -181,6 +181,23 @@ int gdn_cuda_step_host(gdn_cuda_handle *h, double *wn, int nsteps);
  * L2 norm of (w - w_exact).  FP64, deterministic. */
 int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err);
 
+/* No counterpart in the reference.  The same norm as gdn_cuda_error_l2 for
+ * callers that cannot allocate device memory (code running under stream
+ * capture, hosts whose device memory belongs to another allocator or a fixed
+ * start-up budget): it allocates nothing and uses a fixed scratch array of
+ * about 192 KB that every GPU loading the library holds until exit.
+ * Inputs are device pointers the caller owns: w[nbelems*10*6] (the RK3
+ * volume state, reference layout), xyz[nbelems*10*3] (P2 node coordinates),
+ * det[nbelems] (Jacobian determinants); wpg[10] is host memory; *err is
+ * written on the host after `stream` (a cudaStream_t, NULL = legacy stream)
+ * completes.  At most 8,388,608 elements (GDN_CUDA_ERR_INVALID beyond).  All
+ * calls share the scratch: calls that overlap on the GPU race.  The first
+ * call on a device resolves the scratch address and should come before any
+ * stream capture. */
+int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, const double *det, long long nbelems,
+							  const double *wpg, const gdn_cuda_data *data, double t, void *stream,
+							  double *err);
+
 /* ---- introspection ------------------------------------------------------ */
 int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
 /* wlen = m * neq of the reference layout */
