@@ -183,6 +183,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_CUBE, help="cube resolution (default 96)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tile", type=int, default=0, choices=[0, 32, 128],
+                    help="RK3 stage kernel: 32 = warp per field, 128 = thread per element, 0 = auto")
     ap.add_argument("--only", default="both", choices=["both", "fp64", "fp32"],
                     help="profiling aid: run one precision variant only")
     args = ap.parse_args()
@@ -229,7 +231,8 @@ def main():
     for name, prec, b_s in (("fp64", capi.FP64, 8), ("fp32", capi.FP32, 4)):
         if args.only not in ("both", name):
             continue
-        s = capi.Solver(mesh, capi.SCHEME_RK3, data, dt, precision=prec, device=local)
+        s = capi.Solver(mesh, capi.SCHEME_RK3, data, dt, precision=prec, device=local,
+                        elems_per_cta=args.tile)
         st = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
         s.init()
         s.advance(W)

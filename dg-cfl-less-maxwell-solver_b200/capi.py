@@ -227,7 +227,7 @@ class Solver:
 
     def __init__(self, mesh: MeshArrays, scheme=SCHEME_RK3, data: Data = None, dt: float = None,
                  precision=FP64, nb_v=4, tables: Tables = None, device=0, use_graph=1,
-                 refine_passes=1, theta=0.5):
+                 refine_passes=1, theta=0.5, elems_per_cta=0):
         self.L = lib()
         self.mesh = mesh
         self.scheme = scheme
@@ -244,7 +244,7 @@ class Solver:
             model = Model(SCHEME_KINETIC, 6, nb_v, lam, RELAX_OMEGA, _dp(self._vi), theta)
             self.m = 6 * nb_v
         self.nb_v = nb_v
-        cfg = Config(precision, refine_passes, 0, use_graph, device)
+        cfg = Config(precision, refine_passes, elems_per_cta, use_graph, device)
         self.h = C.c_void_p()
         check(self.L.gdn_cuda_attach(C.byref(mesh.struct), C.byref(self.tables), C.byref(model),
                                      C.byref(self.data), C.byref(cfg), float(dt), C.byref(self.h)))

@@ -89,7 +89,9 @@ struct gdn_cuda_handle {
 	// RK3
 	void *w[2] = {nullptr, nullptr};
 	void *k2 = nullptr;
+	void *btrace = nullptr; // [nbf][6][6] boundary traces at the stage time
 	int cur = 0;
+	int rk3_variant = 0; // 0: field-per-warp tiles of 32, 1: element-per-thread tiles of 128
 	// kinetic
 	void *f = nullptr, *y = nullptr, *G = nullptr, *sown = nullptr, *coef = nullptr;
 	int *items = nullptr;
@@ -151,6 +153,18 @@ static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
 	for (int i = 0; i < 6; i++)
 		for (int j = 0; j < 6; j++)
 			o.S[i][j] = (T)t->face_scal[i][j];
+	for (int i = 0; i < 10; i++)
+		for (int j = 0; j < 10; j++) {
+			o.D01[i][j].x = o.D[0][i][j];
+			o.D01[i][j].y = o.D[1][i][j];
+		}
+	for (int m = 0; m < 5; m++)
+		for (int j = 0; j < 10; j++) {
+			o.D2p[m][j].x = o.D[2][2 * m][j];
+			o.D2p[m][j].y = o.D[2][2 * m + 1][j];
+			o.MinvP[m][j].x = o.Minv[2 * m][j];
+			o.MinvP[m][j].y = o.Minv[2 * m + 1][j];
+		}
 	o.n3scale = (T)(t->ref_normal[3][0] * std::sqrt(3.0));
 	for (int f = 0; f < 4; f++) {
 		for (int k = 0; k < 3; k++)
@@ -417,6 +431,12 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		h->neq = 10 * ne + 6 * nbf;
 		GDN_TRY(prepare_rk3<double>());
 		GDN_TRY(prepare_rk3<float>());
+		GDN_TRY(prepare_rk3_ept<double>());
+		GDN_TRY(prepare_rk3_ept<float>());
+		if (fp64)
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->btrace), 36 * (nbf > 0 ? nbf : 1)));
+		else
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->btrace), 36 * (nbf > 0 ? nbf : 1)));
 		for (int b = 0; b < 2; b++) {
 			if (fp64)
 				GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->w[b]), 60 * ne));
@@ -518,6 +538,13 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 	h->scheme = model->scheme;
 	h->precision = cfg.precision;
 	h->use_graph = cfg.use_graph;
+	if (cfg.elems_per_cta != 0 && cfg.elems_per_cta != 32 && cfg.elems_per_cta != 128) {
+		delete h;
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: elems_per_cta must be 0 (auto), 32 or 128");
+	}
+	// RK3 stage kernel: 32-element tiles with a warp per field, or 128-element
+	// tiles with a thread per element
+	h->rk3_variant = cfg.elems_per_cta == 128 ? 1 : 0;
 	h->ne = mesh->nbelems;
 	h->nf = mesh->nbfaces;
 	h->nbf = mesh->nboundaryfaces;
@@ -579,6 +606,7 @@ static int rk3_step(gdn_cuda_handle *h)
 		p.nb = h->nb;
 		p.perm = h->perm;
 		p.bxyz = h->bxyz;
+		p.btrace = as<T>(h->btrace);
 		p.data = h->data;
 		p.ne = h->ne;
 		p.t_stage = h->t + RK_C[i] * h->dt;
@@ -588,7 +616,14 @@ static int rk3_step(gdn_cuda_handle *h)
 		p.stage0 = i == 0;
 		p.write_k2 = i < 2;
 		p.sparse = h->rk3_sparse;
-		GDN_TRY(launch_rk3_stage<T>(p, h->stream));
+		if (h->nbf > 0) {
+			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, h->data, p.t_stage, as<T>(h->btrace), h->stream));
+			h->launches++;
+		}
+		if (h->rk3_variant == 1)
+			GDN_TRY(launch_rk3_stage_ept<T>(p, h->stream));
+		else
+			GDN_TRY(launch_rk3_stage<T>(p, h->stream));
 		h->launches++;
 		h->cur = 1 - h->cur;
 		h->t_bdof = p.t_stage;

@@ -178,6 +178,35 @@ __global__ void boundary_dofs_kernel(const double *__restrict__ bxyz, long long 
 	}
 }
 
+// RK3 boundary traces at a stage time, in the stage kernels' precision:
+// out[(bf*6 + jj)*6 + c] = w_exact(x_{bf,jj}, t)_c  (dg_update_boundary,
+// dg.c:101-104, evaluated once per stage instead of inside the flux loop)
+template <typename T>
+__global__ void boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Data d, double t,
+									  T *__restrict__ out)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= nbf * 6)
+		return;
+	double x[3] = {bxyz[3 * u], bxyz[3 * u + 1], bxyz[3 * u + 2]}, we[6];
+	exact_w(d, x, t, we);
+	for (int c = 0; c < 6; c++)
+		out[u * 6 + c] = (T)we[c];
+}
+
+template <typename T>
+int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, double t, T *out, cudaStream_t s)
+{
+	if (nbf <= 0)
+		return GDN_CUDA_OK;
+	boundary_trace_kernel<T><<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, d, t, out);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+template int launch_boundary_trace<double>(const double *, long long, const Data &, double, double *,
+										   cudaStream_t);
+template int launch_boundary_trace<float>(const double *, long long, const Data &, double, float *, cudaStream_t);
+
 int launch_boundary_dofs(const double *bxyz, long long nbf, const Data &d, double t, int kinetic,
 						 const KinModel &km, long long neq, double *out, cudaStream_t s)
 {

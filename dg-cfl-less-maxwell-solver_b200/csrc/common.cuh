@@ -14,10 +14,27 @@ constexpr int NQV = 6; // P2 nodes per face
 constexpr int NW = 6; // Maxwell fields (Ex, Ey, Ez, Hx, Hy, Hz)
 constexpr int NV_MAX = 6; // kinetic velocities (d3q4: 4, d3q6: 6)
 
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+	typedef float2 type;
+};
+template <>
+struct Vec2<double> {
+	typedef double2 type;
+};
+
 // Reference-element tables, in constant memory so that warp-uniform indices
 // broadcast.  D[k][i][j] = int d_k(phi_i) phi_j (t10_internal_ref[i][j][k]).
+// The *p / D01 arrays hold the same coefficients as adjacent pairs for the
+// packed FP32x2 FMA: D01[i][j] = (D[0][i][j], D[1][i][j]),
+// D2p[m][j] = (D[2][2m][j], D[2][2m+1][j]), MinvP[m][j] = (Minv[2m][j], Minv[2m+1][j]).
 template <typename T>
 struct Tables {
+	typename Vec2<T>::type D01[NQN][NQN];
+	typename Vec2<T>::type D2p[NQN / 2][NQN];
+	typename Vec2<T>::type MinvP[NQN / 2][NQN];
 	T D[3][NQN][NQN];
 	T Minv[NQN][NQN];
 	T M[NQN][NQN];

@@ -14,6 +14,7 @@ struct Rk3Params {
 	const int *nb; // [ne][4] neighbour element, or -(boundary face + 1)
 	const int *perm; // [ne][4] neighbour local node of face node jj, 4 bits each
 	const double *bxyz; // [nbf][6][3] boundary face-node coordinates
+	const T *btrace; // [nbf][6][6] boundary data at t_stage (boundary_trace_kernel)
 	Data data;
 	long long ne;
 	double t_stage, dt, A, B;
@@ -29,6 +30,12 @@ template <typename T>
 int launch_rk3_stage(const Rk3Params<T> &p, cudaStream_t s);
 template <typename T>
 int prepare_rk3();
+template <typename T>
+int launch_rk3_stage_ept(const Rk3Params<T> &p, cudaStream_t s);
+template <typename T>
+int prepare_rk3_ept();
+template <typename T>
+int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, double t, T *out, cudaStream_t s);
 
 // Kinetic (CFL-less) path.
 template <typename S>

@@ -14,9 +14,10 @@
 //   dw = (1/det) Minv R            (simulation.c:241-243)
 // Face fluxes are computed by each element with its own outward normal; the
 // upwind flux is antisymmetric under (wL, wR, n) -> (wR, wL, -n), so this is
-// the reference's +/- pair up to rounding.  Boundary neighbours take the
-// analytic data at the face-node coordinates (dg_update_boundary,
-// dg.c:76-106), evaluated on the device.
+// the reference's +/- pair up to rounding.  Boundary neighbours read the
+// analytic data at the face-node coordinates and the stage time
+// (dg_update_boundary, dg.c:76-106), written by boundary_trace_kernel just
+// before the stage.
 //
 // Work decomposition (TE = 32 elements per CTA, 6 warps):
 //   A  16-byte coalesced loads of the tile (w, k2, geometry, neighbours) into
@@ -58,6 +59,97 @@ __host__ __device__ constexpr int f2n(int f, int j)
 {
 	constexpr int m[4][6] = {{0, 3, 2, 7, 9, 6}, {0, 1, 3, 4, 8, 7}, {0, 2, 1, 6, 5, 4}, {1, 2, 3, 5, 9, 8}};
 	return m[f][j];
+}
+
+// r[k][i] = sum_j D_k[i][j] w[j] for the three reference directions, with the
+// structural zeros skipped at compile time.
+template <typename T, bool SPARSE>
+__device__ __forceinline__ void ref_derivatives(const Tables<T> &tb, const T w[10], T r[3][10])
+{
+#pragma unroll
+	for (int k = 0; k < 3; k++)
+#pragma unroll
+		for (int i = 0; i < 10; i++) {
+			T acc = T(0);
+#pragma unroll
+			for (int j = 0; j < 10; j++)
+				if (!SPARSE || (dmask(k, i) >> j & 1))
+					acc += tb.D[k][i][j] * w[j];
+			r[k][i] = acc;
+		}
+}
+
+// FP32: the same sums with Blackwell's packed FP32x2 FMA, pairing
+// (r0[i], r1[i]) and (r2[2m], r2[2m+1]); coefficient pairs are stored
+// adjacent in constant memory (Tables<float>::D01, D2p).
+template <>
+__device__ __forceinline__ void ref_derivatives<float, true>(const Tables<float> &tb, const float w[10],
+															 float r[3][10])
+{
+	float2 p01[10], p2[5];
+#pragma unroll
+	for (int i = 0; i < 10; i++)
+		p01[i] = make_float2(0.f, 0.f);
+#pragma unroll
+	for (int m = 0; m < 5; m++)
+		p2[m] = make_float2(0.f, 0.f);
+#pragma unroll
+	for (int j = 0; j < 10; j++) {
+		const float2 wd = make_float2(w[j], w[j]);
+#pragma unroll
+		for (int i = 0; i < 10; i++)
+			if ((dmask(0, i) | dmask(1, i)) >> j & 1)
+				p01[i] = __ffma2_rn(tb.D01[i][j], wd, p01[i]);
+#pragma unroll
+		for (int m = 0; m < 5; m++)
+			if ((dmask(2, 2 * m) | dmask(2, 2 * m + 1)) >> j & 1)
+				p2[m] = __ffma2_rn(tb.D2p[m][j], wd, p2[m]);
+	}
+#pragma unroll
+	for (int i = 0; i < 10; i++) {
+		r[0][i] = p01[i].x;
+		r[1][i] = p01[i].y;
+	}
+#pragma unroll
+	for (int m = 0; m < 5; m++) {
+		r[2][2 * m] = p2[m].x;
+		r[2][2 * m + 1] = p2[m].y;
+	}
+}
+
+// dw = Minv R (dense 10 x 10)
+template <typename T>
+__device__ __forceinline__ void lift_minv(const Tables<T> &tb, const T R[10], T dw[10])
+{
+#pragma unroll
+	for (int i = 0; i < 10; i++) {
+		T acc = T(0);
+#pragma unroll
+		for (int j = 0; j < 10; j++)
+			acc += tb.Minv[i][j] * R[j];
+		dw[i] = acc;
+	}
+}
+
+template <>
+__device__ __forceinline__ void lift_minv<float>(const Tables<float> &tb, const float R[10], float dw[10])
+{
+	float2 acc[5];
+#pragma unroll
+	for (int m = 0; m < 5; m++)
+		acc[m] = make_float2(0.f, 0.f);
+#pragma unroll
+	for (int j = 0; j < 10; j++) {
+		const float2 rd = make_float2(R[j], R[j]);
+#pragma unroll
+		for (int m = 0; m < 5; m++)
+			acc[m] = __ffma2_rn(tb.MinvP[m][j], rd, acc[m]);
+	}
+#pragma unroll
+	for (int m = 0; m < 5; m++) {
+		dw[2 * m] = acc[m].x;
+		dw[2 * m + 1] = acc[m].y;
+	}
 }
 
 constexpr int kRk3Tile = 32; // elements per CTA
@@ -123,19 +215,24 @@ __global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
 			sPm[tid] = p.perm[e0 * 4 + tid];
 		}
 	}
-	// out-of-tile neighbour traces of this thread's flux slots (face node
-	// jj = warp of faces 0..3), issued before the barrier so that their
-	// latency overlaps the tile load
+	__syncthreads();
+
+	const int e = lane;
+	const bool live = e < nloc;
+
+	// out-of-tile neighbour traces (or boundary data at the stage time) of this
+	// thread's flux slots -- face node jj = warp of faces 0..3 -- issued now
+	// and consumed after the volume phase, which hides their latency
 	T pre[4][6];
-	if (lane < nloc) {
+	if (live) {
 		const int jj = warp;
 #pragma unroll
 		for (int f = 0; f < 4; f++) {
-			const int nbv = __ldg(p.nb + (e0 + lane) * 4 + f);
+			const int nbv = sNb[e * 4 + f];
 			const long long le = nbv - e0;
-			if (nbv >= 0 && (le < 0 || le >= nloc)) {
-				const int qn = (__ldg(p.perm + (e0 + lane) * 4 + f) >> (4 * jj)) & 15;
-				const T *g = p.w_in + (long long)nbv * 60 + qn * 6;
+			if (nbv < 0 || le < 0 || le >= nloc) {
+				const T *g = nbv >= 0 ? p.w_in + (long long)nbv * 60 + ((sPm[e * 4 + f] >> (4 * jj)) & 15) * 6
+									  : p.btrace + ((long long)(-nbv - 1) * 6 + jj) * 6;
 #pragma unroll
 				for (int c = 0; c < 6; c++)
 					pre[f][c] = __ldg(g + c);
@@ -144,61 +241,6 @@ __global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
 				for (int c = 0; c < 6; c++)
 					pre[f][c] = T(0);
 			}
-		}
-	}
-	__syncthreads();
-
-	const int e = lane;
-	const bool live = e < nloc;
-
-	// ---- B: upwind flux; warp w takes face node jj = w of the 4 faces ----
-	if (live) {
-		const int jj = warp;
-		T cod[3][3];
-#pragma unroll
-		for (int r = 0; r < 3; r++)
-#pragma unroll
-			for (int q = 0; q < 3; q++)
-				cod[r][q] = sG[(3 * r + q) * P + e];
-#pragma unroll
-		for (int f = 0; f < 4; f++) {
-			const int s = 6 * f + jj;
-			const int qo = tb.f2n[f][jj]; // warp-uniform: constant-cache broadcast
-			T wL[6], wR[6], vn[3], F[6];
-#pragma unroll
-			for (int c = 0; c < 6; c++)
-				wL[c] = sW[(qo * 6 + c) * P + e];
-			const int nbv = sNb[e * 4 + f];
-			if (nbv >= 0) {
-				const long long le = nbv - e0;
-				if (le >= 0 && le < nloc) {
-					const int qn = (sPm[e * 4 + f] >> (4 * jj)) & 15;
-#pragma unroll
-					for (int c = 0; c < 6; c++)
-						wR[c] = sW[(qn * 6 + c) * P + (int)le];
-				} else {
-#pragma unroll
-					for (int c = 0; c < 6; c++)
-						wR[c] = pre[f][c];
-				}
-			} else {
-				const double *x = p.bxyz + ((long long)(-nbv - 1) * 6 + jj) * 3;
-				double xx[3] = {x[0], x[1], x[2]}, we[6];
-				exact_w(p.data, xx, p.t_stage, we);
-#pragma unroll
-				for (int c = 0; c < 6; c++)
-					wR[c] = (T)we[c];
-			}
-			// own scaled outward normal codtau . n_ref(f): the reference
-			// normals are -e_0, -e_1, -e_2 and (1,1,1)/sqrt(3), face 3 scaled by
-			// sqrt(3) (simulation.c:377-395; checked at attach)
-#pragma unroll
-			for (int a2 = 0; a2 < 3; a2++)
-				vn[a2] = f < 3 ? -cod[a2][f] : (cod[a2][0] + cod[a2][1] + cod[a2][2]) * tb.n3scale;
-			upwind_flux<T>(wL, wR, vn, F);
-#pragma unroll
-			for (int c = 0; c < 6; c++)
-				sF[(s * 6 + c) * P + e] = F[c];
 		}
 	}
 
@@ -223,22 +265,57 @@ __global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
 			cd1[k] = d1 == 0 ? cod[0][k] : (d1 == 1 ? cod[1][k] : cod[2][k]);
 			cd2[k] = d2 == 0 ? cod[0][k] : (d2 == 1 ? cod[1][k] : cod[2][k]);
 		}
+		T r[3][10];
+		ref_derivatives<T, SPARSE>(tb, w, r);
 #pragma unroll
 		for (int i = 0; i < 10; i++) {
-			T r[3];
-#pragma unroll
-			for (int k = 0; k < 3; k++) {
-				T acc = T(0);
-#pragma unroll
-				for (int j = 0; j < 10; j++)
-					if (!SPARSE || (dmask(k, i) >> j & 1))
-						acc += tb.D[k][i][j] * w[j];
-				r[k] = acc;
-			}
-			sX[((c * 2 + 0) * 10 + i) * P + e] = cd1[0] * r[0] + cd1[1] * r[1] + cd1[2] * r[2];
-			sX[((c * 2 + 1) * 10 + i) * P + e] = cd2[0] * r[0] + cd2[1] * r[1] + cd2[2] * r[2];
+			sX[((c * 2 + 0) * 10 + i) * P + e] = cd1[0] * r[0][i] + cd1[1] * r[1][i] + cd1[2] * r[2][i];
+			sX[((c * 2 + 1) * 10 + i) * P + e] = cd2[0] * r[0][i] + cd2[1] * r[1][i] + cd2[2] * r[2][i];
 		}
 	}
+
+	// ---- B: upwind flux; warp w takes face node jj = w of the 4 faces ----
+	if (live) {
+		const int jj = warp;
+		T cod[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; r++)
+#pragma unroll
+			for (int q = 0; q < 3; q++)
+				cod[r][q] = sG[(3 * r + q) * P + e];
+#pragma unroll
+		for (int f = 0; f < 4; f++) {
+			const int s = 6 * f + jj;
+			const int qo = tb.f2n[f][jj]; // warp-uniform: constant-cache broadcast
+			T wL[6], wR[6], vn[3], F[6];
+#pragma unroll
+			for (int c = 0; c < 6; c++)
+				wL[c] = sW[(qo * 6 + c) * P + e];
+			const int nbv = sNb[e * 4 + f];
+			const long long le = nbv - e0;
+			if (nbv >= 0 && le >= 0 && le < nloc) {
+				const int qn = (sPm[e * 4 + f] >> (4 * jj)) & 15;
+#pragma unroll
+				for (int c = 0; c < 6; c++)
+					wR[c] = sW[(qn * 6 + c) * P + (int)le];
+			} else {
+#pragma unroll
+				for (int c = 0; c < 6; c++)
+					wR[c] = pre[f][c];
+			}
+			// own scaled outward normal codtau . n_ref(f): the reference
+			// normals are -e_0, -e_1, -e_2 and (1,1,1)/sqrt(3), face 3 scaled by
+			// sqrt(3) (simulation.c:377-395; checked at attach)
+#pragma unroll
+			for (int a2 = 0; a2 < 3; a2++)
+				vn[a2] = f < 3 ? -cod[a2][f] : (cod[a2][0] + cod[a2][1] + cod[a2][2]) * tb.n3scale;
+			upwind_flux<T>(wL, wR, vn, F);
+#pragma unroll
+			for (int c = 0; c < 6; c++)
+				sF[(s * 6 + c) * P + e] = F[c];
+		}
+	}
+
 	__syncthreads();
 
 	// ---- D: residual of field c, lift, RK update ----
@@ -270,12 +347,11 @@ __global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
 		}
 		const T inv_det = T(1) / sG[9 * P + e];
 		const T A = (T)p.A, B = (T)p.B, dt = (T)p.dt;
+		T dwv[10];
+		lift_minv<T>(tb, R, dwv);
 #pragma unroll
 		for (int i = 0; i < 10; i++) {
-			T dw = T(0);
-#pragma unroll
-			for (int j = 0; j < 10; j++)
-				dw += tb.Minv[i][j] * R[j];
+			const T dw = dwv[i];
 			const int o = (i * 6 + c) * P + e;
 			const T k2 = (p.stage0 ? T(0) : A * sK[o]) - dt * (dw * inv_det);
 			sK[o] = k2;
