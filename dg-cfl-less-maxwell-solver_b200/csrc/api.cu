@@ -14,8 +14,11 @@
 namespace gdn {
 template <typename GT>
 int launch_kin_setup(const int *face2elem, long long nf, const double *geom, const int *nb, long long ne,
-					 const KinModel &km, double theta_dt, GT *sown, double *sown64, unsigned char *mask, GT *G,
-					 GT *coef, int *bad, cudaStream_t s);
+					 const KinModel &km, double *sown64, unsigned char *mask, cudaStream_t s);
+template <typename GT>
+int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
+					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *coef,
+					  int4 *rnb, int4 *rpm, GT *rs, int *relem, int *bad, cudaStream_t s);
 }
 
 using namespace gdn;
@@ -92,10 +95,18 @@ struct gdn_cuda_handle {
 	void *btrace = nullptr; // [nbf][6][6] boundary traces at the stage time
 	int cur = 0;
 	int rk3_variant = 0; // 0: field-per-warp tiles of 32, 1: element-per-thread tiles of 128
-	// kinetic
-	void *f = nullptr, *y = nullptr, *G = nullptr, *sown = nullptr, *coef = nullptr;
-	int *items = nullptr;
+	// kinetic, in sweep order (item k = position in the level-sorted list)
+	void *f = nullptr, *y = nullptr, *G = nullptr, *coef = nullptr;
+	void *rs = nullptr; // [k][4] own-side v.vn
+	int4 *rnb = nullptr, *rpm = nullptr; // [k] inflow neighbour items, permutations
+	int *relem = nullptr; // [k] element
+	int *items = nullptr; // [k] e * nv + v
+	int *pos = nullptr; // [e * nv + v] k
 	std::vector<int> level_off;
+	// device time and captured step loops
+	double *t_dev = nullptr;
+	cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+	long long graph_nodes[2] = {0, 0};
 };
 
 template <typename X>
@@ -125,6 +136,9 @@ static void free_handle(gdn_cuda_handle *h)
 	cudaSetDevice(h->device);
 	if (h->stream)
 		cudaStreamSynchronize(h->stream);
+	for (int k = 0; k < 2; k++)
+		if (h->graph_exec[k])
+			cudaGraphExecDestroy(h->graph_exec[k]);
 	for (auto &b : h->bufs)
 		cudaFree(b.p);
 	if (h->host_result)
@@ -308,9 +322,11 @@ static int build_neighbours(const gdn_cuda_mesh *m, const gdn_cuda_tables *t, st
 	return GDN_CUDA_OK;
 }
 
-// host Kahn scheduling of the upwind DAG per velocity; items grouped by level
+// host Kahn scheduling of the upwind DAG per velocity; items grouped by
+// level (items[k] = e * nv + v, pos its inverse)
 static int build_schedule(gdn_cuda_handle *h, const std::vector<unsigned char> &mask,
-						  const std::vector<int> &nbv, std::vector<int> &items, std::vector<int> &off)
+						  const std::vector<int> &nbv, std::vector<int> &items, std::vector<int> &pos,
+						  std::vector<int> &off)
 {
 	const long long ne = h->ne;
 	const int nv = h->nv;
@@ -361,9 +377,13 @@ static int build_schedule(gdn_cuda_handle *h, const std::vector<unsigned char> &
 	for (int l = 0; l < nl; l++)
 		off[l + 1] += off[l];
 	items.assign(ne * nv, 0);
-	std::vector<int> pos(off.begin(), off.end() - 1);
-	for (long long u = 0; u < ne * nv; u++)
-		items[pos[level[u]]++] = (int)u;
+	pos.assign(ne * nv, 0);
+	std::vector<int> next(off.begin(), off.end() - 1);
+	for (long long u = 0; u < ne * nv; u++) {
+		const int k = next[level[u]]++;
+		items[k] = (int)u;
+		pos[u] = k;
+	}
 	return GDN_CUDA_OK;
 }
 
@@ -398,6 +418,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 	h->nblk_err = 1184; // 8 x 148 SMs
 	GDN_TRY(dalloc(h, &h->partial, 6 * h->nblk_err));
 	GDN_TRY(dalloc(h, &h->result, 8));
+	GDN_TRY(dalloc(h, &h->t_dev, 1));
 	GDN_CUDA_TRY(cudaMallocHost(&h->host_result, 8 * sizeof(double)));
 	cudaStream_t s = h->stream;
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->e2q, m->elem2qnode, 10 * ne * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -452,43 +473,52 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 	} else {
 		const int nv = h->nv;
 		h->neq = 10 * ne + 6 * nbf;
+		const long long nu = ne * nv;
 		double *sown64;
 		unsigned char *mask;
-		GDN_TRY(dalloc(h, &sown64, 4 * ne * nv));
-		GDN_TRY(dalloc(h, &mask, ne * nv));
+		GDN_TRY(dalloc(h, &sown64, 4 * nu));
+		GDN_TRY(dalloc(h, &mask, nu));
+		// upwind masks first: the schedule (and with it the sweep order every
+		// other kinetic array is stored in) is built on the host from them
+		GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, sown64, mask, s));
+		h->launches += 2;
+		std::vector<unsigned char> hmask(nu);
+		GDN_CUDA_TRY(cudaMemcpyAsync(hmask.data(), mask, nu, cudaMemcpyDeviceToHost, s));
+		GDN_CUDA_TRY(cudaStreamSynchronize(s));
+		std::vector<int> items, pos;
+		GDN_TRY(build_schedule(h, hmask, nb, items, pos, h->level_off));
+		GDN_TRY(dalloc(h, &h->items, nu));
+		GDN_TRY(dalloc(h, &h->pos, nu));
+		GDN_TRY(dalloc(h, &h->rnb, nu));
+		GDN_TRY(dalloc(h, &h->rpm, nu));
+		GDN_TRY(dalloc(h, &h->relem, nu));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->items, items.data(), nu * sizeof(int), cudaMemcpyHostToDevice, s));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->pos, pos.data(), nu * sizeof(int), cudaMemcpyHostToDevice, s));
 		if (fp64) {
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->G), 100 * ne * nv));
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->sown), 4 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->G), 100 * nu));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->rs), 4 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->coef), ne));
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * ne * nv));
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->y), 60 * ne * nv));
-			GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->theta * h->dt,
-											 as<double>(h->sown), sown64, mask, as<double>(h->G),
-											 as<double>(h->coef), h->flag, s));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * nu));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->y), 60 * nu));
+			GDN_TRY(launch_kin_blocks<double>(h->geom64, sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
+											  h->theta * h->dt, as<double>(h->G), as<double>(h->coef), h->rnb,
+											  h->rpm, as<double>(h->rs), h->relem, h->flag, s));
 		} else {
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->G), 100 * ne * nv));
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->sown), 4 * ne * nv));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->G), 100 * nu));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->rs), 4 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->coef), ne));
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->f), 60 * ne * nv));
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->y), 60 * ne * nv));
-			GDN_TRY(launch_kin_setup<float>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->theta * h->dt,
-											as<float>(h->sown), sown64, mask, as<float>(h->G), as<float>(h->coef),
-											h->flag, s));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->f), 60 * nu));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->y), 60 * nu));
+			GDN_TRY(launch_kin_blocks<float>(h->geom64, sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
+											 h->theta * h->dt, as<float>(h->G), as<float>(h->coef), h->rnb, h->rpm,
+											 as<float>(h->rs), h->relem, h->flag, s));
 		}
-		h->launches += 3;
-		std::vector<unsigned char> hmask(ne * nv);
-		GDN_CUDA_TRY(cudaMemcpyAsync(hmask.data(), mask, ne * nv, cudaMemcpyDeviceToHost, s));
+		h->launches += 2;
 		GDN_CUDA_TRY(cudaMemcpyAsync(&bad, h->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
 		GDN_CUDA_TRY(cudaStreamSynchronize(s));
 		if (bad)
 			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: a transport diagonal block is singular");
-		std::vector<int> items;
-		GDN_TRY(build_schedule(h, hmask, nb, items, h->level_off));
-		GDN_TRY(dalloc(h, &h->items, items.size()));
-		GDN_CUDA_TRY(cudaMemcpyAsync(h->items, items.data(), items.size() * sizeof(int), cudaMemcpyHostToDevice,
-									 s));
 		GDN_TRY(dalloc(h, &h->staging, (long long)6 * nv * h->neq));
-		GDN_CUDA_TRY(cudaStreamSynchronize(s));
 	}
 	return GDN_CUDA_OK;
 }
@@ -594,13 +624,14 @@ static const double RK_A[3] = {0., -5. / 9., -153. / 128.};
 static const double RK_B[3] = {1. / 3., 15. / 16., 8. / 15.};
 static const double RK_C[3] = {0., 1. / 3., 3. / 4.};
 
+// ---- enqueue one time step (no host bookkeeping; capturable) ----
 template <typename T>
-static int rk3_step(gdn_cuda_handle *h)
+static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 {
 	for (int i = 0; i < 3; i++) {
 		Rk3Params<T> p;
-		p.w_in = as<T>(h->w[h->cur]);
-		p.w_out = as<T>(h->w[1 - h->cur]);
+		p.w_in = as<T>(h->w[cur]);
+		p.w_out = as<T>(h->w[1 - cur]);
 		p.k2 = as<T>(h->k2);
 		p.geom = reinterpret_cast<const T *>(h->geomT);
 		p.nb = h->nb;
@@ -609,7 +640,6 @@ static int rk3_step(gdn_cuda_handle *h)
 		p.btrace = as<T>(h->btrace);
 		p.data = h->data;
 		p.ne = h->ne;
-		p.t_stage = h->t + RK_C[i] * h->dt;
 		p.dt = h->dt;
 		p.A = RK_A[i];
 		p.B = RK_B[i];
@@ -617,37 +647,39 @@ static int rk3_step(gdn_cuda_handle *h)
 		p.write_k2 = i < 2;
 		p.sparse = h->rk3_sparse;
 		if (h->nbf > 0) {
-			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, h->data, p.t_stage, as<T>(h->btrace), h->stream));
-			h->launches++;
+			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, h->data, h->t_dev, RK_C[i], h->dt, as<T>(h->btrace),
+											 h->stream));
+			nlaunch++;
 		}
 		if (h->rk3_variant == 1)
 			GDN_TRY(launch_rk3_stage_ept<T>(p, h->stream));
 		else
 			GDN_TRY(launch_rk3_stage<T>(p, h->stream));
-		h->launches++;
-		h->cur = 1 - h->cur;
-		h->t_bdof = p.t_stage;
+		nlaunch++;
+		cur = 1 - cur;
 	}
-	h->t += h->dt;
-	h->steps++;
+	GDN_TRY(launch_advance_time(h->t_dev, h->dt, h->stream));
+	nlaunch++;
 	return GDN_CUDA_OK;
 }
 
 template <typename T>
-static int kin_step(gdn_cuda_handle *h)
+static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 {
 	KinSweepParams<T> p;
 	p.f = as<T>(h->f);
 	p.y = as<T>(h->y);
 	p.G = h->G;
-	p.sown = h->sown;
-	p.nb = h->nb;
-	p.perm = h->perm;
+	p.rnb = h->rnb;
+	p.rpm = h->rpm;
+	p.rs = h->rs;
+	p.relem = h->relem;
 	p.bxyz = h->bxyz;
 	p.coef = h->coef;
 	p.items = h->items;
 	p.data = h->data;
-	p.t_half = h->t + h->dt / 2;
+	p.t_dev = h->t_dev;
+	p.dt = h->dt;
 	for (int i = 0; i < 3 * NV_MAX; i++)
 		p.vi[i] = h->km.vi[i];
 	p.feq_c = h->km.feq_c;
@@ -657,11 +689,12 @@ static int kin_step(gdn_cuda_handle *h)
 		p.item_begin = h->level_off[l];
 		p.item_end = h->level_off[l + 1];
 		GDN_TRY((launch_kin_sweep<T, T>(p, h->stream)));
-		h->launches++;
+		nlaunch++;
 	}
 	KinRelaxParams<T> r;
 	r.f = as<T>(h->f);
 	r.y = as<T>(h->y);
+	r.pos = h->pos;
 	r.ne = h->ne;
 	r.nv = h->nv;
 	for (int i = 0; i < 3 * NV_MAX; i++)
@@ -670,29 +703,84 @@ static int kin_step(gdn_cuda_handle *h)
 	r.omega = h->omega;
 	r.a_y = 1.0 / h->theta;
 	r.a_f = -(1.0 - h->theta) / h->theta;
-	r.two_over_theta_minus = 0;
 	GDN_TRY(launch_kin_relax<T>(r, h->stream));
-	h->launches++;
+	nlaunch++;
+	GDN_TRY(launch_advance_time(h->t_dev, h->dt, h->stream));
+	nlaunch++;
+	return GDN_CUDA_OK;
+}
+
+static int enqueue_steps(gdn_cuda_handle *h, int nsteps, int &cur, long long &nlaunch)
+{
+	for (int n = 0; n < nsteps; n++) {
+		if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(rk3_enqueue<double>(h, cur, nlaunch));
+			else
+				GDN_TRY(rk3_enqueue<float>(h, cur, nlaunch));
+		} else {
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(kin_enqueue<double>(h, nlaunch));
+			else
+				GDN_TRY(kin_enqueue<float>(h, nlaunch));
+		}
+	}
+	return GDN_CUDA_OK;
+}
+
+// host mirror of the device time, as the reference accumulates it
+static void bookkeep_step(gdn_cuda_handle *h)
+{
+	h->t_bdof = h->t + RK_C[2] * h->dt;
 	h->t += h->dt;
 	h->steps++;
+}
+
+// Step loops as CUDA graphs: RK3 captures 2 steps (6 stages: the ping-pong
+// buffers come back to the same parity), one graph per starting parity; the
+// level-launch kinetic step captures 1 step.  Everything a step reads that
+// changes from step to step (the time) lives on the device.
+static int capture_graph(gdn_cuda_handle *h, int key, int unit)
+{
+	cudaGraph_t graph = nullptr;
+	GDN_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+	int cur = key;
+	long long nl = 0;
+	int rc = enqueue_steps(h, unit, cur, nl);
+	cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+	if (rc != GDN_CUDA_OK)
+		return rc;
+	if (ce != cudaSuccess)
+		return gdn_cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+	ce = cudaGraphInstantiate(&h->graph_exec[key], graph, 0);
+	cudaGraphDestroy(graph);
+	if (ce != cudaSuccess)
+		return gdn_cuda_fail(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+	h->graph_nodes[key] = nl;
 	return GDN_CUDA_OK;
 }
 
 static int advance_impl(gdn_cuda_handle *h, int nsteps)
 {
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
-	for (int n = 0; n < nsteps; n++) {
-		if (h->scheme == GDN_CUDA_SCHEME_RK3) {
-			if (h->precision == GDN_CUDA_FP64)
-				GDN_TRY(rk3_step<double>(h));
-			else
-				GDN_TRY(rk3_step<float>(h));
-		} else {
-			if (h->precision == GDN_CUDA_FP64)
-				GDN_TRY(kin_step<double>(h));
-			else
-				GDN_TRY(kin_step<float>(h));
-		}
+	const bool graphable = h->use_graph != 0;
+	const int unit = h->scheme == GDN_CUDA_SCHEME_RK3 ? 2 : 1;
+	while (graphable && nsteps >= unit) {
+		const int key = h->scheme == GDN_CUDA_SCHEME_RK3 ? h->cur : 0;
+		if (!h->graph_exec[key])
+			GDN_TRY(capture_graph(h, key, unit));
+		GDN_CUDA_TRY(cudaGraphLaunch(h->graph_exec[key], h->stream));
+		for (int u = 0; u < unit; u++)
+			bookkeep_step(h);
+		h->launches += h->graph_nodes[key];
+		nsteps -= unit;
+	}
+	while (nsteps > 0) {
+		long long nl = 0;
+		GDN_TRY(enqueue_steps(h, 1, h->cur, nl));
+		h->launches += nl;
+		bookkeep_step(h);
+		nsteps--;
 	}
 	return GDN_CUDA_OK;
 }
@@ -719,10 +807,12 @@ extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
 		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
 	} else {
 		if (h->precision == GDN_CUDA_FP64)
-			GDN_TRY(launch_init_kin<double>(h->e2q, h->node, h->ne, h->data, h->km, as<double>(h->f), s));
+			GDN_TRY(launch_init_kin<double>(h->e2q, h->node, h->ne, h->data, h->km, h->pos, as<double>(h->f), s));
 		else
-			GDN_TRY(launch_init_kin<float>(h->e2q, h->node, h->ne, h->data, h->km, as<float>(h->f), s));
+			GDN_TRY(launch_init_kin<float>(h->e2q, h->node, h->ne, h->data, h->km, h->pos, as<float>(h->f), s));
 	}
+	h->launches++;
+	GDN_TRY(launch_set_time(h->t_dev, 0.0, s));
 	h->launches++;
 	h->t = 0.0;
 	h->t_bdof = 0.0;
@@ -753,11 +843,13 @@ extern "C" int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t
 		const long long wl = (long long)6 * h->nv * h->neq;
 		GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, wl * sizeof(double), cudaMemcpyHostToDevice, s));
 		if (h->precision == GDN_CUDA_FP64)
-			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), ne, h->nv, h->neq, h->staging, 0, s));
+			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 0, s));
 		else
-			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), ne, h->nv, h->neq, h->staging, 0, s));
+			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 0, s));
 		h->launches++;
 	}
+	GDN_TRY(launch_set_time(h->t_dev, t, s));
+	h->launches++;
 	h->t = t;
 	h->t_bdof = t;
 	return GDN_CUDA_OK;
@@ -784,9 +876,9 @@ static int get_state_impl(gdn_cuda_handle *h, double *wn)
 		// boundary dofs after dg_update_boundary(simu, t) (relaxation.c:175)
 		GDN_TRY(launch_boundary_dofs(h->bxyz, h->nbf, h->data, h->t, 1, h->km, h->neq, h->staging + 10 * ne, s));
 		if (h->precision == GDN_CUDA_FP64)
-			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), ne, h->nv, h->neq, h->staging, 1, s));
+			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 1, s));
 		else
-			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), ne, h->nv, h->neq, h->staging, 1, s));
+			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 1, s));
 		h->launches += 2;
 		GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, (long long)6 * h->nv * h->neq * sizeof(double),
 									 cudaMemcpyDeviceToHost, s));
@@ -839,11 +931,11 @@ extern "C" int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err)
 	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
 	const void *st = kin ? h->f : h->w[h->cur];
 	if (h->precision == GDN_CUDA_FP64)
-		GDN_TRY(launch_error_l2<double>(as<double>(const_cast<void *>(st)), kin, h->nv, h->e2q, h->node,
+		GDN_TRY(launch_error_l2<double>(as<double>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q, h->node,
 										h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
 	else
-		GDN_TRY(launch_error_l2<float>(as<float>(const_cast<void *>(st)), kin, h->nv, h->e2q, h->node, h->geom64,
-									   h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
+		GDN_TRY(launch_error_l2<float>(as<float>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q, h->node,
+									   h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
 	h->launches += 2;
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->host_result, h->result, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
 	GDN_CUDA_TRY(cudaStreamSynchronize(s));

@@ -118,10 +118,10 @@ __device__ __forceinline__ void feq_component(const double w[6], const double *v
 }
 
 // dg_init_sol_macro, kinetic branch: f = f_eq(w_exact(x, 0)); layout
-// f[e][v][c][i]
+// f[k][c][i] with k = pos[e * nv + v] (sweep order)
 template <typename S>
 __global__ void init_kin_kernel(const int *__restrict__ e2q, const double *__restrict__ node, long long ne,
-								Data d, KinModel km, S *__restrict__ f)
+								Data d, KinModel km, const int *__restrict__ pos, S *__restrict__ f)
 {
 	const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (t >= ne * 10)
@@ -134,24 +134,24 @@ __global__ void init_kin_kernel(const int *__restrict__ e2q, const double *__res
 	for (int v = 0; v < km.nv; v++) {
 		feq_component(we, km.vi + 3 * v, km.nv, km.feq_c, fe);
 		for (int c = 0; c < 6; c++)
-			Store<S>::store(f + ((e * km.nv + v) * 6 + c) * 10 + i, fe[c]);
+			Store<S>::store(f + ((long long)pos[e * km.nv + v] * 6 + c) * 10 + i, fe[c]);
 	}
 }
 
 template <typename S>
-int launch_init_kin(const int *e2q, const double *node, long long ne, const Data &d, const KinModel &km, S *f,
-					cudaStream_t s)
+int launch_init_kin(const int *e2q, const double *node, long long ne, const Data &d, const KinModel &km,
+					const int *pos, S *f, cudaStream_t s)
 {
-	init_kin_kernel<S><<<(unsigned)((ne * 10 + 255) / 256), 256, 0, s>>>(e2q, node, ne, d, km, f);
+	init_kin_kernel<S><<<(unsigned)((ne * 10 + 255) / 256), 256, 0, s>>>(e2q, node, ne, d, km, pos, f);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
 template int launch_init_kin<double>(const int *, const double *, long long, const Data &, const KinModel &,
-									 double *, cudaStream_t);
+									 const int *, double *, cudaStream_t);
 template int launch_init_kin<float>(const int *, const double *, long long, const Data &, const KinModel &,
-									float *, cudaStream_t);
+									const int *, float *, cudaStream_t);
 template int launch_init_kin<__nv_bfloat16>(const int *, const double *, long long, const Data &,
-											const KinModel &, __nv_bfloat16 *, cudaStream_t);
+											const KinModel &, const int *, __nv_bfloat16 *, cudaStream_t);
 
 // Boundary dofs of the reference layout.  RK3: w_exact(x_L, t)
 // (dg_update_boundary, dg.c:101-104); kinetic: f_eq(w_exact(x_L, t))
@@ -181,13 +181,18 @@ __global__ void boundary_dofs_kernel(const double *__restrict__ bxyz, long long 
 // RK3 boundary traces at a stage time, in the stage kernels' precision:
 // out[(bf*6 + jj)*6 + c] = w_exact(x_{bf,jj}, t)_c  (dg_update_boundary,
 // dg.c:101-104, evaluated once per stage instead of inside the flux loop)
+// The stage time t + C_i dt is formed from the device copy of t with the
+// host's rounding (no fused multiply-add), so every stage sees the
+// reference's time bits.
 template <typename T>
-__global__ void boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Data d, double t,
+__global__ void boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Data d,
+									  const double *__restrict__ t_dev, double c_stage, double dt,
 									  T *__restrict__ out)
 {
 	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (u >= nbf * 6)
 		return;
+	const double t = __dadd_rn(*t_dev, __dmul_rn(c_stage, dt));
 	double x[3] = {bxyz[3 * u], bxyz[3 * u + 1], bxyz[3 * u + 2]}, we[6];
 	exact_w(d, x, t, we);
 	for (int c = 0; c < 6; c++)
@@ -195,17 +200,43 @@ __global__ void boundary_trace_kernel(const double *__restrict__ bxyz, long long
 }
 
 template <typename T>
-int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, double t, T *out, cudaStream_t s)
+int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double c_stage,
+						  double dt, T *out, cudaStream_t s)
 {
 	if (nbf <= 0)
 		return GDN_CUDA_OK;
-	boundary_trace_kernel<T><<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, d, t, out);
+	boundary_trace_kernel<T><<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, d, t_dev, c_stage, dt,
+																				out);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_boundary_trace<double>(const double *, long long, const Data &, double, double *,
-										   cudaStream_t);
-template int launch_boundary_trace<float>(const double *, long long, const Data &, double, float *, cudaStream_t);
+template int launch_boundary_trace<double>(const double *, long long, const Data &, const double *, double, double,
+										   double *, cudaStream_t);
+template int launch_boundary_trace<float>(const double *, long long, const Data &, const double *, double, double,
+										  float *, cudaStream_t);
+
+// device time: t = value, and t += dt (the reference's accumulation,
+// explicit.c:103 / relaxation.c:171)
+__global__ void set_time_kernel(double *t, double value)
+{
+	*t = value;
+}
+__global__ void advance_time_kernel(double *t, double dt)
+{
+	*t = __dadd_rn(*t, dt);
+}
+int launch_set_time(double *t, double value, cudaStream_t s)
+{
+	set_time_kernel<<<1, 1, 0, s>>>(t, value);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+int launch_advance_time(double *t, double dt, cudaStream_t s)
+{
+	advance_time_kernel<<<1, 1, 0, s>>>(t, dt);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
 
 int launch_boundary_dofs(const double *bxyz, long long nbf, const Data &d, double t, int kinetic,
 						 const KinModel &km, long long neq, double *out, cudaStream_t s)
@@ -218,10 +249,11 @@ int launch_boundary_dofs(const double *bxyz, long long nbf, const Data &d, doubl
 	return GDN_CUDA_OK;
 }
 
-// kinetic device layout f[e][v][c][i]  <->  wn[(c*nv + v)*neq + 10 e + i]
+// kinetic device layout f[k][c][i], k = pos[e * nv + v]
+//   <->  wn[(c*nv + v)*neq + 10 e + i]
 template <typename S>
-__global__ void kin_pack_kernel(const S *__restrict__ f, long long ne, int nv, long long neq,
-								double *__restrict__ wn, int to_ref)
+__global__ void kin_pack_kernel(const S *__restrict__ f, const int *__restrict__ pos, long long ne, int nv,
+								long long neq, double *__restrict__ wn, int to_ref)
 {
 	const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	const long long tot = ne * nv * 60;
@@ -233,30 +265,34 @@ __global__ void kin_pack_kernel(const S *__restrict__ f, long long ne, int nv, l
 	const int v = (int)(ev % nv);
 	const long long e = ev / nv;
 	const long long r = (long long)(c * nv + v) * neq + e * 10 + i;
+	const long long o = (long long)pos[ev] * 60 + c * 10 + i;
 	if (to_ref)
-		wn[r] = (double)Store<S>::load(f + t);
+		wn[r] = (double)Store<S>::load(f + o);
 	else
-		Store<S>::store(const_cast<S *>(f) + t, wn[r]);
+		Store<S>::store(const_cast<S *>(f) + o, wn[r]);
 }
 
 template <typename S>
-int launch_kin_pack(const S *f, long long ne, int nv, long long neq, double *wn, int to_ref, cudaStream_t s)
+int launch_kin_pack(const S *f, const int *pos, long long ne, int nv, long long neq, double *wn, int to_ref,
+					cudaStream_t s)
 {
 	const long long tot = ne * nv * 60;
-	kin_pack_kernel<S><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(f, ne, nv, neq, wn, to_ref);
+	kin_pack_kernel<S><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(f, pos, ne, nv, neq, wn, to_ref);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_kin_pack<double>(const double *, long long, int, long long, double *, int, cudaStream_t);
-template int launch_kin_pack<float>(const float *, long long, int, long long, double *, int, cudaStream_t);
-template int launch_kin_pack<__nv_bfloat16>(const __nv_bfloat16 *, long long, int, long long, double *, int,
-											cudaStream_t);
+template int launch_kin_pack<double>(const double *, const int *, long long, int, long long, double *, int,
+									 cudaStream_t);
+template int launch_kin_pack<float>(const float *, const int *, long long, int, long long, double *, int,
+									cudaStream_t);
+template int launch_kin_pack<__nv_bfloat16>(const __nv_bfloat16 *, const int *, long long, int, long long, double *,
+											int, cudaStream_t);
 
 // K2: simulation_error_l2 (src/simulation/simulation.c:606-666).  Pass 1: one
 // FP64 partial per block and field, in a fixed order; pass 2: one block sums
 // the partials in order.  Deterministic for a given launch shape.
 template <typename S>
-__global__ void error_partial_kernel(const S *__restrict__ state, int kinetic, int nv,
+__global__ void error_partial_kernel(const S *__restrict__ state, int kinetic, int nv, const int *__restrict__ pos,
 									 const int *__restrict__ e2q, const double *__restrict__ node,
 									 const double *__restrict__ geom, long long ne, Data d, double t,
 									 double *__restrict__ partial)
@@ -278,7 +314,7 @@ __global__ void error_partial_kernel(const S *__restrict__ state, int kinetic, i
 			for (int c = 0; c < 6; c++) {
 				double s = 0.0;
 				for (int v = 0; v < nv; v++)
-					s += (double)Store<S>::load(state + ((e * nv + v) * 6 + c) * 10 + i);
+					s += (double)Store<S>::load(state + ((long long)pos[e * nv + v] * 6 + c) * 10 + i);
 				wl[c] = s;
 			}
 		}
@@ -329,22 +365,24 @@ __global__ void error_final_kernel(const double *__restrict__ partial, int nblk,
 }
 
 template <typename S>
-int launch_error_l2(const S *state, int kinetic, int nv, const int *e2q, const double *node, const double *geom,
-					long long ne, const Data &d, double t, double *partial, int nblk, double *out,
+int launch_error_l2(const S *state, int kinetic, int nv, const int *pos, const int *e2q, const double *node,
+					const double *geom, long long ne, const Data &d, double t, double *partial, int nblk, double *out,
 					cudaStream_t s)
 {
-	error_partial_kernel<S><<<nblk, 256, 0, s>>>(state, kinetic, nv, e2q, node, geom, ne, d, t, partial);
+	error_partial_kernel<S><<<nblk, 256, 0, s>>>(state, kinetic, nv, pos, e2q, node, geom, ne, d, t, partial);
 	GDN_CUDA_TRY(cudaGetLastError());
 	error_final_kernel<<<1, 256, 0, s>>>(partial, nblk, out);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_error_l2<double>(const double *, int, int, const int *, const double *, const double *,
-									 long long, const Data &, double, double *, int, double *, cudaStream_t);
-template int launch_error_l2<float>(const float *, int, int, const int *, const double *, const double *,
-									long long, const Data &, double, double *, int, double *, cudaStream_t);
-template int launch_error_l2<__nv_bfloat16>(const __nv_bfloat16 *, int, int, const int *, const double *,
-											const double *, long long, const Data &, double, double *, int,
-											double *, cudaStream_t);
+template int launch_error_l2<double>(const double *, int, int, const int *, const int *, const double *,
+									 const double *, long long, const Data &, double, double *, int, double *,
+									 cudaStream_t);
+template int launch_error_l2<float>(const float *, int, int, const int *, const int *, const double *,
+									const double *, long long, const Data &, double, double *, int, double *,
+									cudaStream_t);
+template int launch_error_l2<__nv_bfloat16>(const __nv_bfloat16 *, int, int, const int *, const int *,
+											const double *, const double *, long long, const Data &, double, double *,
+											int, double *, cudaStream_t);
 
 } // namespace gdn

@@ -159,22 +159,29 @@ __device__ __forceinline__ void maxwell_A(const T n[3], const T w[6], T out[6])
 // Storage conversions for the state (FP64 / FP32 / BF16 storage).
 template <typename S>
 struct Store;
+// load_l2 bypasses L1 (data written by other SMs during the same launch).
 template <>
 struct Store<double> {
 	typedef double compute;
 	__device__ __forceinline__ static double load(const double *p) { return *p; }
+	__device__ __forceinline__ static double load_l2(const double *p) { return __ldcg(p); }
 	__device__ __forceinline__ static void store(double *p, double v) { *p = v; }
 };
 template <>
 struct Store<float> {
 	typedef float compute;
 	__device__ __forceinline__ static float load(const float *p) { return *p; }
+	__device__ __forceinline__ static float load_l2(const float *p) { return __ldcg(p); }
 	__device__ __forceinline__ static void store(float *p, float v) { *p = v; }
 };
 template <>
 struct Store<__nv_bfloat16> {
 	typedef float compute;
 	__device__ __forceinline__ static float load(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+	__device__ __forceinline__ static float load_l2(const __nv_bfloat16 *p)
+	{
+		return __bfloat162float(__ushort_as_bfloat16(__ldcg(reinterpret_cast<const unsigned short *>(p))));
+	}
 	__device__ __forceinline__ static void store(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
 };
 

@@ -84,3 +84,47 @@ def test_kinetic_fp64_matches_golden_fixture(name, nb_v):
     rel = np.linalg.norm(wn - g[key + "_wn"]) / np.linalg.norm(g[key + "_wn"])
     assert rel <= 1e-12, rel
     assert t == float(g[key + "_t"])
+
+
+def _vol_mask(s, mesh):
+    """True on the volume dofs of the kinetic reference layout
+    wn[(iw * nb_v + iv) * neq + ipg] (ipg < 10 * nbelems)."""
+    neq = s.wlen // (6 * s.nb_v)
+    m = np.zeros((6 * s.nb_v, neq), bool)
+    m[:, : 10 * mesh.nbelems] = True
+    return m.ravel()
+
+
+def test_kinetic_state_round_trip_through_sweep_order():
+    """set_state scatters the reference layout into the device's sweep order
+    and get_state gathers it back: volume dofs come back bit for bit."""
+    c, e = kuhn.kuhn_cube(5, 0.1, seed=4)
+    mesh = capi.mesh_build(c, e)
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), 3 * mesh.hmin(), nb_v=6)
+    rng = np.random.default_rng(3)
+    wn = rng.standard_normal(s.wlen)
+    s.set_state(wn, 0.25)
+    back = s.get_state()
+    m = _vol_mask(s, mesh)
+    s.close()
+    assert np.array_equal(back[m], wn[m])
+
+
+def test_kinetic_step_host_equals_device_resident_steps():
+    """gdn_cuda_step_host (host state in/out) gives the same state as
+    advancing on the device."""
+    c, e = kuhn.kuhn_cube(4, 0.1, seed=2)
+    mesh = capi.mesh_build(c, e)
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), 3 * mesh.hmin())
+    s.init()
+    s.advance(3)
+    w3 = s.get_state()
+    t3 = s.t
+    s.advance(4)
+    w7 = s.get_state()
+    host = w3.copy()
+    s.set_state(host, t3)
+    s.step_host(host, 4)
+    m = _vol_mask(s, mesh)
+    s.close()
+    assert np.array_equal(host[m], w7[m])
