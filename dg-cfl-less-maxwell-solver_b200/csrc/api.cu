@@ -17,8 +17,8 @@ int launch_kin_setup(const int *face2elem, long long nf, const double *geom, con
 					 const KinModel &km, double *sown64, unsigned char *mask, cudaStream_t s);
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
-					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *coef,
-					  int4 *rnb, int4 *rpm, GT *rs, int *relem, int *bad, cudaStream_t s);
+					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *rcoef,
+					  int4 *rnb, int4 *rpm, GT *rs, int *bad, cudaStream_t s);
 }
 
 using namespace gdn;
@@ -96,10 +96,16 @@ struct gdn_cuda_handle {
 	int cur = 0;
 	int rk3_variant = 0; // 0: field-per-warp tiles of 32, 1: element-per-thread tiles of 128
 	// kinetic, in sweep order (item k = position in the level-sorted list)
-	void *f = nullptr, *y = nullptr, *G = nullptr, *coef = nullptr;
+	// f: FP64 (FP64, FP32_REFINE), FP32 or BF16; y: FP64 or FP32; G, rs,
+	// rcoef: FP64 (FP64) or FP32
+	void *f = nullptr, *y = nullptr, *G = nullptr, *rcoef = nullptr;
 	void *rs = nullptr; // [k][4] own-side v.vn
 	int4 *rnb = nullptr, *rpm = nullptr; // [k] inflow neighbour items, permutations
-	int *relem = nullptr; // [k] element
+	double *bt = nullptr; // [bf][v][6][6] boundary f_eq at t + dt/2
+	double *sown64 = nullptr; // [e * nv + v][4] v.vn in FP64 (refinement residual)
+	double *yacc = nullptr; // FP32_REFINE: FP64 solution of the transport solve
+	float *rhs = nullptr; // FP32_REFINE: residual, right-hand side of the corrections
+	int refine_passes = 1;
 	int *items = nullptr; // [k] e * nv + v
 	int *pos = nullptr; // [e * nv + v] k
 	std::vector<int> level_off;
@@ -474,13 +480,12 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		const int nv = h->nv;
 		h->neq = 10 * ne + 6 * nbf;
 		const long long nu = ne * nv;
-		double *sown64;
 		unsigned char *mask;
-		GDN_TRY(dalloc(h, &sown64, 4 * nu));
+		GDN_TRY(dalloc(h, &h->sown64, 4 * nu));
 		GDN_TRY(dalloc(h, &mask, nu));
 		// upwind masks first: the schedule (and with it the sweep order every
 		// other kinetic array is stored in) is built on the host from them
-		GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, sown64, mask, s));
+		GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->sown64, mask, s));
 		h->launches += 2;
 		std::vector<unsigned char> hmask(nu);
 		GDN_CUDA_TRY(cudaMemcpyAsync(hmask.data(), mask, nu, cudaMemcpyDeviceToHost, s));
@@ -491,27 +496,36 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		GDN_TRY(dalloc(h, &h->pos, nu));
 		GDN_TRY(dalloc(h, &h->rnb, nu));
 		GDN_TRY(dalloc(h, &h->rpm, nu));
-		GDN_TRY(dalloc(h, &h->relem, nu));
+		GDN_TRY(dalloc(h, &h->bt, 36LL * nv * (nbf > 0 ? nbf : 1)));
 		GDN_CUDA_TRY(cudaMemcpyAsync(h->items, items.data(), nu * sizeof(int), cudaMemcpyHostToDevice, s));
 		GDN_CUDA_TRY(cudaMemcpyAsync(h->pos, pos.data(), nu * sizeof(int), cudaMemcpyHostToDevice, s));
+		// state f: FP64 for FP64 and FP32_REFINE, FP32, or BF16
+		if (h->precision == GDN_CUDA_FP64 || h->precision == GDN_CUDA_FP32_REFINE)
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * nu));
+		else if (h->precision == GDN_CUDA_FP32)
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->f), 60 * nu));
+		else
+			GDN_TRY(dalloc(h, reinterpret_cast<__nv_bfloat16 **>(&h->f), 60 * nu));
 		if (fp64) {
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->G), 100 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->rs), 4 * nu));
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->coef), ne));
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * nu));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->rcoef), nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->y), 60 * nu));
-			GDN_TRY(launch_kin_blocks<double>(h->geom64, sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
-											  h->theta * h->dt, as<double>(h->G), as<double>(h->coef), h->rnb,
-											  h->rpm, as<double>(h->rs), h->relem, h->flag, s));
+			GDN_TRY(launch_kin_blocks<double>(h->geom64, h->sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
+											  h->theta * h->dt, as<double>(h->G), as<double>(h->rcoef), h->rnb,
+											  h->rpm, as<double>(h->rs), h->flag, s));
 		} else {
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->G), 100 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->rs), 4 * nu));
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->coef), ne));
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->f), 60 * nu));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->rcoef), nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->y), 60 * nu));
-			GDN_TRY(launch_kin_blocks<float>(h->geom64, sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
-											 h->theta * h->dt, as<float>(h->G), as<float>(h->coef), h->rnb, h->rpm,
-											 as<float>(h->rs), h->relem, h->flag, s));
+			GDN_TRY(launch_kin_blocks<float>(h->geom64, h->sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
+											 h->theta * h->dt, as<float>(h->G), as<float>(h->rcoef), h->rnb, h->rpm,
+											 as<float>(h->rs), h->flag, s));
+		}
+		if (h->precision == GDN_CUDA_FP32_REFINE) {
+			GDN_TRY(dalloc(h, &h->yacc, 60 * nu));
+			GDN_TRY(dalloc(h, &h->rhs, 60 * nu));
 		}
 		h->launches += 2;
 		GDN_CUDA_TRY(cudaMemcpyAsync(&bad, h->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -552,8 +566,8 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 			return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: kinetic sets d3q4 (4) or d3q6 (6) only");
 		if (!model->vi || !(model->lambda > 0.0) || !(model->theta > 0.0) || !(model->theta <= 1.0))
 			return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kinetic model needs vi, lambda > 0, 0 < theta <= 1");
-		if (cfg.precision > GDN_CUDA_FP32)
-			return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: precision mode not built for the kinetic path");
+		if (cfg.precision == GDN_CUDA_FP32_REFINE && (cfg.refine_passes < 0 || cfg.refine_passes > 4))
+			return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: refine_passes must be in [0, 4]");
 	}
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -567,6 +581,7 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 	h->device = cfg.device;
 	h->scheme = model->scheme;
 	h->precision = cfg.precision;
+	h->refine_passes = cfg.refine_passes;
 	h->use_graph = cfg.use_graph;
 	if (cfg.elems_per_cta != 0 && cfg.elems_per_cta != 32 && cfg.elems_per_cta != 128) {
 		delete h;
@@ -663,37 +678,38 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 	return GDN_CUDA_OK;
 }
 
-template <typename T>
-static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
+// all sweep levels of one transport solve M1 y = f
+template <typename F, typename Y, typename T>
+static int kin_sweeps(gdn_cuda_handle *h, const void *f, int acc, int bdata, long long &nlaunch)
 {
-	KinSweepParams<T> p;
-	p.f = as<T>(h->f);
-	p.y = as<T>(h->y);
+	KinSweepParams p;
+	p.f = f;
+	p.y = h->y;
+	p.yacc = h->yacc;
 	p.G = h->G;
+	p.rs = h->rs;
+	p.rcoef = h->rcoef;
 	p.rnb = h->rnb;
 	p.rpm = h->rpm;
-	p.rs = h->rs;
-	p.relem = h->relem;
-	p.bxyz = h->bxyz;
-	p.coef = h->coef;
 	p.items = h->items;
-	p.data = h->data;
-	p.t_dev = h->t_dev;
-	p.dt = h->dt;
-	for (int i = 0; i < 3 * NV_MAX; i++)
-		p.vi[i] = h->km.vi[i];
-	p.feq_c = h->km.feq_c;
+	p.bt = h->bt;
 	p.nv = h->nv;
 	const int nl = (int)h->level_off.size() - 1;
 	for (int l = 0; l < nl; l++) {
 		p.item_begin = h->level_off[l];
 		p.item_end = h->level_off[l + 1];
-		GDN_TRY((launch_kin_sweep<T, T>(p, h->stream)));
+		GDN_TRY((launch_kin_sweep<F, Y, T>(p, acc, bdata, h->rk3_sparse, h->stream)));
 		nlaunch++;
 	}
-	KinRelaxParams<T> r;
-	r.f = as<T>(h->f);
-	r.y = as<T>(h->y);
+	return GDN_CUDA_OK;
+}
+
+template <typename F, typename Y, typename T>
+static int kin_relax(gdn_cuda_handle *h, const void *y, long long &nlaunch)
+{
+	KinRelaxParams r;
+	r.f = h->f;
+	r.y = y;
 	r.pos = h->pos;
 	r.ne = h->ne;
 	r.nv = h->nv;
@@ -703,8 +719,59 @@ static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 	r.omega = h->omega;
 	r.a_y = 1.0 / h->theta;
 	r.a_f = -(1.0 - h->theta) / h->theta;
-	GDN_TRY(launch_kin_relax<T>(r, h->stream));
+	GDN_TRY((launch_kin_relax<F, Y, T>(r, h->stream)));
 	nlaunch++;
+	return GDN_CUDA_OK;
+}
+
+// one CFL-less step: boundary f_eq at t + dt/2, the transport solve of every
+// velocity (level sweeps), the relaxation, t += dt
+static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
+{
+	if (h->nbf > 0) {
+		GDN_TRY(launch_kin_boundary_trace(h->bxyz, h->nbf, h->data, h->t_dev, h->dt, h->nv, h->km.vi, h->km.feq_c,
+										  h->bt, h->stream));
+		nlaunch++;
+	}
+	switch (h->precision) {
+	case GDN_CUDA_FP64:
+		GDN_TRY((kin_sweeps<double, double, double>(h, h->f, 0, 1, nlaunch)));
+		GDN_TRY((kin_relax<double, double, double>(h, h->y, nlaunch)));
+		break;
+	case GDN_CUDA_FP32:
+		GDN_TRY((kin_sweeps<float, float, float>(h, h->f, 0, 1, nlaunch)));
+		GDN_TRY((kin_relax<float, float, float>(h, h->y, nlaunch)));
+		break;
+	case GDN_CUDA_BF16_STORE:
+		GDN_TRY((kin_sweeps<__nv_bfloat16, float, float>(h, h->f, 0, 1, nlaunch)));
+		GDN_TRY((kin_relax<__nv_bfloat16, float, float>(h, h->y, nlaunch)));
+		break;
+	default: { // GDN_CUDA_FP32_REFINE
+		GDN_TRY((kin_sweeps<double, float, float>(h, h->f, 1, 1, nlaunch)));
+		KinResidualParams q;
+		q.f = as<double>(h->f);
+		q.yacc = h->yacc;
+		q.r = h->rhs;
+		q.rnb = h->rnb;
+		q.rpm = h->rpm;
+		q.items = h->items;
+		q.sown64 = h->sown64;
+		q.geom = h->geom64;
+		q.bt = h->bt;
+		q.theta_dt = h->theta * h->dt;
+		for (int i = 0; i < 3 * NV_MAX; i++)
+			q.vi[i] = h->km.vi[i];
+		q.nv = h->nv;
+		q.nitems = h->ne * h->nv;
+		for (int pass = 0; pass < h->refine_passes; pass++) {
+			GDN_TRY(launch_kin_residual(q, h->rk3_sparse, h->stream));
+			nlaunch++;
+			GDN_TRY((kin_sweeps<float, float, float>(h, h->rhs, 2, 0, nlaunch)));
+		}
+		GDN_TRY((kin_relax<double, double, double>(h, h->yacc, nlaunch)));
+		break;
+	}
+	}
 	GDN_TRY(launch_advance_time(h->t_dev, h->dt, h->stream));
 	nlaunch++;
 	return GDN_CUDA_OK;
@@ -719,10 +786,7 @@ static int enqueue_steps(gdn_cuda_handle *h, int nsteps, int &cur, long long &nl
 			else
 				GDN_TRY(rk3_enqueue<float>(h, cur, nlaunch));
 		} else {
-			if (h->precision == GDN_CUDA_FP64)
-				GDN_TRY(kin_enqueue<double>(h, nlaunch));
-			else
-				GDN_TRY(kin_enqueue<float>(h, nlaunch));
+			GDN_TRY(kin_enqueue(h, nlaunch));
 		}
 	}
 	return GDN_CUDA_OK;
@@ -792,6 +856,28 @@ extern "C" int gdn_cuda_advance(gdn_cuda_handle *h, int nsteps)
 	return advance_impl(h, nsteps);
 }
 
+// storage type of the kinetic distributions: 0 FP64, 1 FP32, 2 BF16
+static int kin_state_kind(const gdn_cuda_handle *h)
+{
+	if (h->precision == GDN_CUDA_FP32)
+		return 1;
+	if (h->precision == GDN_CUDA_BF16_STORE)
+		return 2;
+	return 0;
+}
+
+// kinetic state <-> reference layout in the staging buffer
+static int kin_pack(gdn_cuda_handle *h, int to_ref)
+{
+	const int sk = kin_state_kind(h);
+	if (sk == 0)
+		return launch_kin_pack<double>(as<double>(h->f), h->pos, h->ne, h->nv, h->neq, h->staging, to_ref, h->stream);
+	if (sk == 1)
+		return launch_kin_pack<float>(as<float>(h->f), h->pos, h->ne, h->nv, h->neq, h->staging, to_ref, h->stream);
+	return launch_kin_pack<__nv_bfloat16>(as<__nv_bfloat16>(h->f), h->pos, h->ne, h->nv, h->neq, h->staging, to_ref,
+										  h->stream);
+}
+
 extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
 {
 	if (!h)
@@ -806,10 +892,14 @@ extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
 			GDN_TRY(launch_init_rk3<float>(h->e2q, h->node, h->ne, h->data, as<float>(h->w[0]), s));
 		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
 	} else {
-		if (h->precision == GDN_CUDA_FP64)
+		const int sk = kin_state_kind(h);
+		if (sk == 0)
 			GDN_TRY(launch_init_kin<double>(h->e2q, h->node, h->ne, h->data, h->km, h->pos, as<double>(h->f), s));
-		else
+		else if (sk == 1)
 			GDN_TRY(launch_init_kin<float>(h->e2q, h->node, h->ne, h->data, h->km, h->pos, as<float>(h->f), s));
+		else
+			GDN_TRY(launch_init_kin<__nv_bfloat16>(h->e2q, h->node, h->ne, h->data, h->km, h->pos,
+												   as<__nv_bfloat16>(h->f), s));
 	}
 	h->launches++;
 	GDN_TRY(launch_set_time(h->t_dev, 0.0, s));
@@ -842,10 +932,7 @@ extern "C" int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t
 	} else {
 		const long long wl = (long long)6 * h->nv * h->neq;
 		GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, wl * sizeof(double), cudaMemcpyHostToDevice, s));
-		if (h->precision == GDN_CUDA_FP64)
-			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 0, s));
-		else
-			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 0, s));
+		GDN_TRY(kin_pack(h, 0));
 		h->launches++;
 	}
 	GDN_TRY(launch_set_time(h->t_dev, t, s));
@@ -875,10 +962,7 @@ static int get_state_impl(gdn_cuda_handle *h, double *wn)
 	} else {
 		// boundary dofs after dg_update_boundary(simu, t) (relaxation.c:175)
 		GDN_TRY(launch_boundary_dofs(h->bxyz, h->nbf, h->data, h->t, 1, h->km, h->neq, h->staging + 10 * ne, s));
-		if (h->precision == GDN_CUDA_FP64)
-			GDN_TRY(launch_kin_pack<double>(as<double>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 1, s));
-		else
-			GDN_TRY(launch_kin_pack<float>(as<float>(h->f), h->pos, ne, h->nv, h->neq, h->staging, 1, s));
+		GDN_TRY(kin_pack(h, 1));
 		h->launches += 2;
 		GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, (long long)6 * h->nv * h->neq * sizeof(double),
 									 cudaMemcpyDeviceToHost, s));
@@ -930,12 +1014,17 @@ extern "C" int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err)
 	cudaStream_t s = h->stream;
 	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
 	const void *st = kin ? h->f : h->w[h->cur];
-	if (h->precision == GDN_CUDA_FP64)
+	const int sk = kin ? kin_state_kind(h) : (h->precision == GDN_CUDA_FP64 ? 0 : 1);
+	if (sk == 0)
 		GDN_TRY(launch_error_l2<double>(as<double>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q, h->node,
 										h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
-	else
+	else if (sk == 1)
 		GDN_TRY(launch_error_l2<float>(as<float>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q, h->node,
 									   h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
+	else
+		GDN_TRY(launch_error_l2<__nv_bfloat16>(as<__nv_bfloat16>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q,
+											   h->node, h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err,
+											   h->result, s));
 	h->launches += 2;
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->host_result, h->result, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
 	GDN_CUDA_TRY(cudaStreamSynchronize(s));

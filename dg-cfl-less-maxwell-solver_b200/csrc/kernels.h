@@ -40,38 +40,55 @@ int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, cons
 int launch_set_time(double *t, double value, cudaStream_t s);
 int launch_advance_time(double *t, double dt, cudaStream_t s);
 
-// Kinetic (CFL-less) path.
-template <typename S>
+// Kinetic (CFL-less) path.  The kinetic state is stored in sweep order: item
+// k (its position in the level-sorted list of (element, velocity) pairs)
+// owns f[k*60 .. +60], y[k*60 ..], G[k*100 ..]; within an item the layout is
+// [field c][node i].
 struct KinSweepParams {
-	// The kinetic state is stored in sweep order: item k (its position in the
-	// level-sorted list of (element, velocity) pairs) owns f[k*60 .. +60],
-	// y[k*60 ..], G[k*100 ..], laid out [field c][node i].
-	const S *f; // distributions at the start of the step
-	S *y; // y = M1^-1 f (written level by level)
-	const void *G; // block inverses (GT)
+	const void *f; // right-hand side of M1 y = f (F)
+	void *y; // solution, written level by level; read back as the inflow traces (Y)
+	double *yacc; // refinement: FP64 solution, = y (ACC 1) or += y (ACC 2)
+	const void *G; // [k][10][10] inverse of the M1 diagonal block (T)
+	const void *rs; // [k][4] own-side v.vn per face (T)
+	const void *rcoef; // [k] theta dt / det (T)
 	const int4 *rnb; // [k] per face: inflow neighbour item, -(bf + 1) inflow boundary face, INT_MIN none
 	const int4 *rpm; // [k] per face: neighbour local node of face node jj, 4 bits each
-	const void *rs; // [k][4] own-side v.vn per face (GT)
-	const int *relem; // [k] element of item k
-	const double *bxyz; // [nbf][6][3]
-	const void *coef; // [ne] theta dt / det (GT)
 	const int *items; // [k] e * nv + v
-	Data data;
-	const double *t_dev; // current time t on the device; boundary data at t + dt/2
-	double dt;
-	double vi[3 * NV_MAX];
-	double feq_c; // f_eq = w / nv + feq_c A(v) w
+	const double *bt; // [bf][v][c][jj] f_eq of the boundary data at t + dt/2
 	int nv;
 	int item_begin, item_end;
 };
 
-template <typename S, typename GT>
-int launch_kin_sweep(const KinSweepParams<S> &p, cudaStream_t s);
+// f: F, y: Y, arithmetic and G: T.  acc: 0 none, 1 yacc = y, 2 yacc += y.
+// bdata: inflow boundary faces take bt (0: zero boundary data, for
+// correction solves).
+template <typename F, typename Y, typename T>
+int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cudaStream_t s);
 
-template <typename S>
+// f_eq of the analytic data at the boundary face nodes, t + dt/2 (FP64)
+int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double dt,
+							  int nv, const double *vi, double feq_c, double *bt, cudaStream_t s);
+
+// FP64 residual r = f - b - M1 yacc of every item (b: inflow boundary data)
+struct KinResidualParams {
+	const double *f;
+	const double *yacc;
+	float *r;
+	const int4 *rnb, *rpm;
+	const int *items;
+	const double *sown64; // [e * nv + v][4]
+	const double *geom; // [e][10] FP64
+	const double *bt;
+	double theta_dt;
+	double vi[3 * NV_MAX];
+	int nv;
+	long long nitems;
+};
+int launch_kin_residual(const KinResidualParams &p, int sparse, cudaStream_t s);
+
 struct KinRelaxParams {
-	S *f; // in: f^n, out: f^{n+1} (sweep order)
-	const S *y;
+	void *f; // in: f^n, out: f^{n+1} (F, sweep order)
+	const void *y; // (Y)
 	const int *pos; // [e * nv + v] item index k of (e, v)
 	long long ne;
 	int nv;
@@ -79,7 +96,7 @@ struct KinRelaxParams {
 	double feq_c, omega;
 	double a_y, a_f; // x = a_y y + a_f f  (2, -1 for theta = 1/2)
 };
-template <typename S>
-int launch_kin_relax(const KinRelaxParams<S> &p, cudaStream_t s);
+template <typename F, typename Y, typename T>
+int launch_kin_relax(const KinRelaxParams &p, cudaStream_t s);
 
 } // namespace gdn

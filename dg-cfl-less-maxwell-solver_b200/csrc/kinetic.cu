@@ -20,8 +20,14 @@
 // Sweep order: the state of (element e, velocity v) lives at item index
 // k = pos[e * nv + v], its position in the level-sorted item list, so the
 // items of one level are contiguous in memory and an item finds everything
-// it needs from one record (inflow neighbour items, permutations, v . vn).
+// it needs in its records (inflow neighbour items, permutations, v . vn,
+// theta dt / det).
+//
+// Mixed precision (GDN_CUDA_FP32_REFINE): FP64 state, FP32 sweeps, FP64
+// residual r = f - b - M1 y computed matrix-free from the FP64 geometry, then
+// FP32 correction sweeps M1 d = r with zero boundary data, y += d.
 #include <climits>
+#include <type_traits>
 
 #include <cuda_pipeline_primitives.h>
 
@@ -70,11 +76,11 @@ __global__ void kin_mask_kernel(const double *__restrict__ sown64, const int *__
 }
 
 // G = D^-1 per (element, velocity), FP64 Gauss-Jordan with partial
-// pivoting, written at the item's sweep position.
+// pivoting, written at the item's sweep position with theta dt / det.
 template <typename GT>
 __global__ void kin_blocks_kernel(const double *__restrict__ geom, const double *__restrict__ sown64,
 								  const int *__restrict__ pos, long long ne, KinModel km, double theta_dt,
-								  GT *__restrict__ G, GT *__restrict__ coef, int *__restrict__ bad)
+								  GT *__restrict__ G, GT *__restrict__ rcoef, int *__restrict__ bad)
 {
 	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (u >= ne * km.nv)
@@ -142,12 +148,12 @@ __global__ void kin_blocks_kernel(const double *__restrict__ geom, const double 
 						a[r][q] -= m * a[k][q];
 			}
 	}
-	GT *Gk = G + (long long)pos[u] * 100;
+	const long long k = pos[u];
+	GT *Gk = G + k * 100;
 	for (int i = 0; i < 10; i++)
 		for (int j = 0; j < 10; j++)
 			Gk[i * 10 + j] = (GT)a[i][10 + j];
-	if (v == 0)
-		coef[e] = (GT)c;
+	rcoef[k] = (GT)c;
 }
 
 // per-item records of the sweep
@@ -155,7 +161,7 @@ template <typename GT>
 __global__ void kin_records_kernel(const int *__restrict__ items, const int *__restrict__ pos,
 								   const double *__restrict__ sown64, const int *__restrict__ nb,
 								   const int *__restrict__ perm, long long nitems, int nv, int4 *__restrict__ rnb,
-								   int4 *__restrict__ rpm, GT *__restrict__ rs, int *__restrict__ relem)
+								   int4 *__restrict__ rpm, GT *__restrict__ rs)
 {
 	const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (k >= nitems)
@@ -178,7 +184,6 @@ __global__ void kin_records_kernel(const int *__restrict__ items, const int *__r
 	}
 	rnb[k] = make_int4(n[0], n[1], n[2], n[3]);
 	rpm[k] = make_int4(pm[0], pm[1], pm[2], pm[3]);
-	relem[k] = (int)e;
 }
 
 template <typename GT>
@@ -195,15 +200,15 @@ int launch_kin_setup(const int *face2elem, long long nf, const double *geom, con
 
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
-					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *coef,
-					  int4 *rnb, int4 *rpm, GT *rs, int *relem, int *bad, cudaStream_t s)
+					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *rcoef,
+					  int4 *rnb, int4 *rpm, GT *rs, int *bad, cudaStream_t s)
 {
 	const long long nu = ne * km.nv;
-	kin_blocks_kernel<GT><<<(unsigned)((nu + 127) / 128), 128, 0, s>>>(geom, sown64, pos, ne, km, theta_dt, G, coef,
+	kin_blocks_kernel<GT><<<(unsigned)((nu + 127) / 128), 128, 0, s>>>(geom, sown64, pos, ne, km, theta_dt, G, rcoef,
 																	   bad);
 	GDN_CUDA_TRY(cudaGetLastError());
 	kin_records_kernel<GT><<<(unsigned)((nu + 255) / 256), 256, 0, s>>>(items, pos, sown64, nb, perm, nu, km.nv, rnb,
-																		rpm, rs, relem);
+																		rpm, rs);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
@@ -211,142 +216,389 @@ template int launch_kin_setup<double>(const int *, long long, const double *, co
 									  const KinModel &, double *, unsigned char *, cudaStream_t);
 template int launch_kin_blocks<double>(const double *, const double *, const int *, const int *, const int *,
 									   const int *, long long, const KinModel &, double, double *, double *, int4 *,
-									   int4 *, double *, int *, int *, cudaStream_t);
+									   int4 *, double *, int *, cudaStream_t);
 template int launch_kin_blocks<float>(const double *, const double *, const int *, const int *, const int *,
 									  const int *, long long, const KinModel &, double, float *, float *, int4 *,
-									  int4 *, float *, int *, int *, cudaStream_t);
+									  int4 *, float *, int *, cudaStream_t);
 
-// One level of the block forward substitution: a warp per item, all 6
-// fields; the items of a level are contiguous.
-constexpr int SWEEP_WARPS = 8;
-
-template <typename S, typename GT>
-__global__ void __launch_bounds__(SWEEP_WARPS * 32) kin_sweep_kernel(KinSweepParams<S> p)
+// f_eq of the analytic data at every boundary face node for every velocity,
+// at t + dt/2 (relaxation.c:99, dg_update_boundary with use_feq), formed from
+// the device time with the host's rounding.  bt[((bf * nv + v) * 6 + c) * 6 + jj].
+__global__ void kin_boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Data d,
+										  const double *__restrict__ t_dev, double dt, KinModel km,
+										  double *__restrict__ bt)
 {
-	typedef GT T;
-	// per warp: inflow traces [face][field][node] (144), lifted face terms
-	// (144), node accumulators (60), right-hand side (60), own f (60), G (100)
-	__shared__ __align__(16) T sh[SWEEP_WARPS][144 + 144 + 60 + 60 + 60 + 100];
-	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-	const long long k = (long long)p.item_begin + (long long)blockIdx.x * SWEEP_WARPS + w;
-	if (k >= p.item_end)
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= nbf * 6)
 		return;
-	const Tables<T> &tb = tab<T>();
-	const int nv = p.nv;
-	T *tr = sh[w], *phi = tr + 144, *tacc = phi + 144, *r = tacc + 60, *fs = r + 60, *gs = fs + 60;
-	// independent data first, copied asynchronously into shared memory while
-	// the trace loads are in flight: own f (60 values) and G (100)
-	{
-		const S *fe = p.f + k * 60;
-		const T *G = reinterpret_cast<const T *>(p.G) + k * 100;
-		constexpr int VG = 16 / sizeof(T);
-		for (int q = l; q < 100 / VG; q += 32)
-			__pipeline_memcpy_async(gs + q * VG, G + q * VG, 16);
-		if (sizeof(S) == sizeof(T)) {
-			for (int q = l; q < 60 / VG; q += 32)
-				__pipeline_memcpy_async(fs + q * VG, reinterpret_cast<const T *>(fe) + q * VG, 16);
-		} else {
-			for (int q = l; q < 60; q += 32)
-				fs[q] = (T)Store<S>::load(fe + q);
-		}
-		__pipeline_commit();
-	}
-	const int4 nb4 = p.rnb[k];
-	const int4 pm4 = p.rpm[k];
-	const int nbk[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
-	const int pmk[4] = {pm4.x, pm4.y, pm4.z, pm4.w};
-	const T *rs = reinterpret_cast<const T *>(p.rs) + k * 4;
-	const int e = p.relem[k];
-	const T coef = reinterpret_cast<const T *>(p.coef)[e];
-	const int v = p.items[k] % nv;
-	// all inflow traces in one round trip: q = (face*6 + field)*6 + node
-	for (int q = l; q < 144; q += 32) {
-		const int f = q / 36, c = (q % 36) / 6, jj = q % 6;
-		const int nbv = f == 0 ? nbk[0] : f == 1 ? nbk[1] : f == 2 ? nbk[2] : nbk[3];
-		const int pm = f == 0 ? pmk[0] : f == 1 ? pmk[1] : f == 2 ? pmk[2] : pmk[3];
-		T val = T(0);
-		if (nbv >= 0) {
-			val = (T)Store<S>::load(p.y + (long long)nbv * 60 + c * 10 + ((pm >> (4 * jj)) & 15));
-		} else if (nbv != INT_MIN) {
-			const double t_half = __dadd_rn(*p.t_dev, __dmul_rn(0.5, p.dt)); // t + dt / 2
-			const double *x = p.bxyz + ((long long)(-nbv - 1) * 6 + jj) * 3;
-			double xx[3] = {x[0], x[1], x[2]}, we[6], Aw[6];
-			exact_w(p.data, xx, t_half, we);
-			double n[3] = {p.vi[3 * v], p.vi[3 * v + 1], p.vi[3 * v + 2]};
-			maxwell_A<double>(n, we, Aw);
-			val = (T)(we[c] / nv + p.feq_c * Aw[c]);
-		}
-		tr[q] = val;
-	}
-	__syncwarp();
-	// phi[f][c][ii] = s_f (S tr[f][c])_ii on inflow faces
-	for (int q = l; q < 144; q += 32) {
-		const int f = q / 36, base = q - q % 6, ii = q % 6;
-		const int nbv = f == 0 ? nbk[0] : f == 1 ? nbk[1] : f == 2 ? nbk[2] : nbk[3];
-		T acc = T(0);
-		if (nbv != INT_MIN) {
-#pragma unroll
-			for (int jj = 0; jj < 6; jj++)
-				acc += tb.S[ii][jj] * tr[base + jj];
-			acc *= rs[f];
-		}
-		phi[q] = acc;
-	}
-	__syncwarp();
-	// gather the face terms at the element nodes
-	for (int q = l; q < 60; q += 32) {
-		const int c = q / 10, i = q % 10;
-		T acc = T(0);
-		for (int a = 0; a < tb.nface_of_node[i]; a++)
-			acc += phi[(tb.face_of_node[i][a] * 6 + c) * 6 + tb.pos_of_node[i][a]];
-		tacc[q] = acc;
-	}
-	__pipeline_wait_prior(0);
-	__syncwarp();
-	for (int q = l; q < 60; q += 32) {
-		const int c = q / 10, i = q % 10;
-		T acc = T(0);
-#pragma unroll
-		for (int j = 0; j < 10; j++)
-			acc += tb.Minv[i][j] * tacc[c * 10 + j];
-		r[q] = fs[q] - coef * acc;
-	}
-	__syncwarp();
-	S *ye = p.y + k * 60;
-	for (int q = l; q < 60; q += 32) {
-		const int c = q / 10, i = q % 10;
-		T acc = T(0);
-#pragma unroll
-		for (int j = 0; j < 10; j++)
-			acc += gs[i * 10 + j] * r[c * 10 + j];
-		Store<S>::store(ye + q, acc);
+	const long long bf = u / 6;
+	const int jj = (int)(u % 6);
+	const double t_half = __dadd_rn(*t_dev, __dmul_rn(0.5, dt));
+	double x[3] = {bxyz[3 * u], bxyz[3 * u + 1], bxyz[3 * u + 2]}, we[6], Aw[6];
+	exact_w(d, x, t_half, we);
+	for (int v = 0; v < km.nv; v++) {
+		double n[3] = {km.vi[3 * v], km.vi[3 * v + 1], km.vi[3 * v + 2]};
+		maxwell_A<double>(n, we, Aw);
+		for (int c = 0; c < 6; c++)
+			bt[((bf * km.nv + v) * 6 + c) * 6 + jj] = we[c] / km.nv + km.feq_c * Aw[c];
 	}
 }
 
-template <typename S, typename GT>
-int launch_kin_sweep(const KinSweepParams<S> &p, cudaStream_t s)
+int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double dt,
+							  int nv, const double *vi, double feq_c, double *bt, cudaStream_t s)
+{
+	if (nbf <= 0)
+		return GDN_CUDA_OK;
+	KinModel km;
+	km.nv = nv;
+	for (int i = 0; i < 3 * NV_MAX; i++)
+		km.vi[i] = vi[i];
+	km.feq_c = feq_c;
+	kin_boundary_trace_kernel<<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, d, t_dev, dt, km, bt);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+
+// 10 consecutive values of one field of one item, converted to T.  The item
+// offsets k*60 + c*10 keep float pairs 8-byte, double pairs 16-byte and
+// bfloat16 pairs 4-byte aligned.
+template <typename S, typename T>
+__device__ __forceinline__ void load10(const S *p, T v[10])
+{
+	if constexpr (std::is_same<S, float>::value) {
+		const float2 *q = reinterpret_cast<const float2 *>(p);
+#pragma unroll
+		for (int i = 0; i < 5; i++) {
+			const float2 a = q[i];
+			v[2 * i] = (T)a.x;
+			v[2 * i + 1] = (T)a.y;
+		}
+	} else if constexpr (std::is_same<S, double>::value) {
+		const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+		for (int i = 0; i < 5; i++) {
+			const double2 a = q[i];
+			v[2 * i] = (T)a.x;
+			v[2 * i + 1] = (T)a.y;
+		}
+	} else {
+		const __nv_bfloat162 *q = reinterpret_cast<const __nv_bfloat162 *>(p);
+#pragma unroll
+		for (int i = 0; i < 5; i++) {
+			const float2 a = __bfloat1622float2(q[i]);
+			v[2 * i] = (T)a.x;
+			v[2 * i + 1] = (T)a.y;
+		}
+	}
+}
+
+template <typename S, typename T>
+__device__ __forceinline__ void store10(S *p, const T v[10])
+{
+	if constexpr (std::is_same<S, float>::value) {
+		float2 *q = reinterpret_cast<float2 *>(p);
+#pragma unroll
+		for (int i = 0; i < 5; i++)
+			q[i] = make_float2((float)v[2 * i], (float)v[2 * i + 1]);
+	} else if constexpr (std::is_same<S, double>::value) {
+		double2 *q = reinterpret_cast<double2 *>(p);
+#pragma unroll
+		for (int i = 0; i < 5; i++)
+			q[i] = make_double2((double)v[2 * i], (double)v[2 * i + 1]);
+	} else {
+		__nv_bfloat162 *q = reinterpret_cast<__nv_bfloat162 *>(p);
+#pragma unroll
+		for (int i = 0; i < 5; i++)
+			q[i] = __floats2bfloat162_rn((float)v[2 * i], (float)v[2 * i + 1]);
+	}
+}
+
+// One level of the block forward substitution.  A CTA takes 32 consecutive
+// items of the level with 6 warps: lane = item, warp = field, so the tables
+// are warp-uniform (constant-bank operands) and every thread owns one field
+// of one item end to end:
+//   traces of the inflow faces (24 independent loads, one round trip),
+//   t = sum_inflow s E_f S tr_f,  r = f - coef Minv t,  y = G r.
+// G of the 32 items is staged by cp.async into shared memory while the
+// traces are in flight; its per-item stride (100 floats / 102 doubles) keeps
+// the 16-byte row reads conflict-free.
+constexpr int kSwItems = 32;
+constexpr int kSwThreads = 6 * 32;
+
+template <typename T>
+struct SweepG {
+	static constexpr int stride = sizeof(T) == 4 ? 100 : 102;
+	typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type vec;
+	static constexpr int per_vec = 16 / sizeof(T);
+};
+
+template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE>
+__global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
+{
+	typedef SweepG<T> SG;
+	__shared__ __align__(16) T gsh[kSwItems * SG::stride];
+	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+	const long long k0 = (long long)p.item_begin + (long long)blockIdx.x * kSwItems;
+	const long long rem = (long long)p.item_end - k0;
+	const int nloc = rem < kSwItems ? (int)rem : kSwItems;
+	{
+		constexpr int VPC = SG::per_vec, CH = 100 / VPC;
+		const T *G = reinterpret_cast<const T *>(p.G) + k0 * 100;
+		for (int q = threadIdx.x; q < nloc * CH; q += kSwThreads) {
+			const int it = q / CH, ch = q - it * CH;
+			__pipeline_memcpy_async(gsh + it * SG::stride + ch * VPC, G + it * 100 + ch * VPC, 16);
+		}
+		__pipeline_commit();
+	}
+	const Tables<T> &tb = tab<T>();
+	const bool act = lane < nloc;
+	const long long k = k0 + lane;
+	T r[10];
+	if (act) {
+		const int4 nb4 = p.rnb[k];
+		const int4 pm4 = p.rpm[k];
+		const int nbk[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+		const int pmk[4] = {pm4.x, pm4.y, pm4.z, pm4.w};
+		const T *rs = reinterpret_cast<const T *>(p.rs) + k * 4;
+		T tr[4][6];
+#pragma unroll
+		for (int f = 0; f < 4; f++) {
+			const int nbv = nbk[f];
+			if (nbv >= 0) {
+				const Y *yn = reinterpret_cast<const Y *>(p.y) + (long long)nbv * 60 + c * 10;
+#pragma unroll
+				for (int jj = 0; jj < 6; jj++)
+					tr[f][jj] = (T)Store<Y>::load(yn + ((pmk[f] >> (4 * jj)) & 15));
+			} else if (BD && nbv != INT_MIN) {
+				const int v = p.items[k] % p.nv;
+				const double *b = p.bt + (((long long)(-nbv - 1) * p.nv + v) * 6 + c) * 6;
+#pragma unroll
+				for (int jj = 0; jj < 6; jj++)
+					tr[f][jj] = (T)b[jj];
+			} else {
+#pragma unroll
+				for (int jj = 0; jj < 6; jj++)
+					tr[f][jj] = T(0);
+			}
+		}
+		T fv[10];
+		load10<F, T>(reinterpret_cast<const F *>(p.f) + k * 60 + c * 10, fv);
+		const T coef = reinterpret_cast<const T *>(p.rcoef)[k];
+		T s[4];
+#pragma unroll
+		for (int f = 0; f < 4; f++)
+			s[f] = rs[f];
+		// t_i = sum over the faces through node i of s_f (S tr_f)_ii
+		T t[10];
+#pragma unroll
+		for (int i = 0; i < 10; i++)
+			t[i] = T(0);
+#pragma unroll
+		for (int f = 0; f < 4; f++) {
+#pragma unroll
+			for (int ii = 0; ii < 6; ii++) {
+				T acc = T(0);
+#pragma unroll
+				for (int jj = 0; jj < 6; jj++)
+					if (!SPARSE || (smask(ii) >> jj & 1))
+						acc += tb.S[ii][jj] * tr[f][jj];
+				t[f2n(f, ii)] += acc * s[f];
+			}
+		}
+#pragma unroll
+		for (int i = 0; i < 10; i++) {
+			T acc = T(0);
+#pragma unroll
+			for (int j = 0; j < 10; j++)
+				acc += tb.Minv[i][j] * t[j];
+			r[i] = fv[i] - coef * acc;
+		}
+	}
+	__pipeline_wait_prior(0);
+	__syncthreads();
+	if (!act)
+		return;
+	T y[10];
+#pragma unroll
+	for (int i = 0; i < 10; i++)
+		y[i] = T(0);
+	const typename SG::vec *g = reinterpret_cast<const typename SG::vec *>(gsh + lane * SG::stride);
+#pragma unroll
+	for (int q = 0; q < 100 / SG::per_vec; q++) {
+		const typename SG::vec gv = g[q];
+		const T *ge = reinterpret_cast<const T *>(&gv);
+#pragma unroll
+		for (int u = 0; u < SG::per_vec; u++) {
+			const int idx = q * SG::per_vec + u;
+			y[idx / 10] += ge[u] * r[idx % 10];
+		}
+	}
+	store10<Y, T>(reinterpret_cast<Y *>(p.y) + k * 60 + c * 10, y);
+	if (ACC) {
+		double *ya = p.yacc + k * 60 + c * 10;
+#pragma unroll
+		for (int i = 0; i < 10; i++)
+			ya[i] = ACC == 1 ? (double)y[i] : ya[i] + (double)y[i];
+	}
+}
+
+template <typename F, typename Y, typename T>
+int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cudaStream_t s)
 {
 	const long long n = (long long)p.item_end - p.item_begin;
 	if (n <= 0)
 		return GDN_CUDA_OK;
-	kin_sweep_kernel<S, GT><<<(unsigned)((n + SWEEP_WARPS - 1) / SWEEP_WARPS), SWEEP_WARPS * 32, 0, s>>>(p);
+	const unsigned grid = (unsigned)((n + kSwItems - 1) / kSwItems);
+#define GDN_SWEEP(A, B, SP) kin_sweep_kernel<F, Y, T, A, B, SP><<<grid, kSwThreads, 0, s>>>(p)
+	if (acc == 0 && bdata) {
+		if (sparse)
+			GDN_SWEEP(0, true, true);
+		else
+			GDN_SWEEP(0, true, false);
+	} else if (acc == 1 && bdata) {
+		if (sparse)
+			GDN_SWEEP(1, true, true);
+		else
+			GDN_SWEEP(1, true, false);
+	} else if (acc == 2 && !bdata) {
+		if (sparse)
+			GDN_SWEEP(2, false, true);
+		else
+			GDN_SWEEP(2, false, false);
+	} else {
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "kinetic sweep: unsupported accumulate / boundary mode");
+	}
+#undef GDN_SWEEP
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_kin_sweep<double, double>(const KinSweepParams<double> &, cudaStream_t);
-template int launch_kin_sweep<float, float>(const KinSweepParams<float> &, cudaStream_t);
+template int launch_kin_sweep<double, double, double>(const KinSweepParams &, int, int, int, cudaStream_t);
+template int launch_kin_sweep<float, float, float>(const KinSweepParams &, int, int, int, cudaStream_t);
+template int launch_kin_sweep<__nv_bfloat16, float, float>(const KinSweepParams &, int, int, int, cudaStream_t);
+template int launch_kin_sweep<double, float, float>(const KinSweepParams &, int, int, int, cudaStream_t);
+
+// FP64 residual of the transport system of every item (no level order: it
+// only reads y), same thread layout as the sweep:
+//   r = f - y - coef Minv (V y + sum_outflow s E S E^T y + sum_inflow s E S tr)
+// with V_ij = -(u . D_ij), u_k = v . codtau[:, k], tr the upwind neighbour's
+// y or the boundary f_eq.  This is f - b - M1 y with M1 exactly as the
+// blocks kernel builds it, in FP64 from the FP64 geometry and v.vn.
+template <bool SPARSE>
+__global__ void __launch_bounds__(kSwThreads) kin_residual_kernel(KinResidualParams p)
+{
+	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+	const long long k = (long long)blockIdx.x * kSwItems + lane;
+	if (k >= p.nitems)
+		return;
+	const Tables<double> &tb = c_tab_d;
+	const long long u = p.items[k];
+	const long long e = u / p.nv;
+	const int v = (int)(u % p.nv);
+	const int4 nb4 = p.rnb[k];
+	const int4 pm4 = p.rpm[k];
+	const int nbk[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+	const int pmk[4] = {pm4.x, pm4.y, pm4.z, pm4.w};
+	double tr[4][6];
+#pragma unroll
+	for (int f = 0; f < 4; f++) {
+		const int nbv = nbk[f];
+		if (nbv >= 0) {
+			const double *yn = p.yacc + (long long)nbv * 60 + c * 10;
+#pragma unroll
+			for (int jj = 0; jj < 6; jj++)
+				tr[f][jj] = yn[(pmk[f] >> (4 * jj)) & 15];
+		} else if (nbv != INT_MIN) {
+			const double *b = p.bt + (((long long)(-nbv - 1) * p.nv + v) * 6 + c) * 6;
+#pragma unroll
+			for (int jj = 0; jj < 6; jj++)
+				tr[f][jj] = b[jj];
+		} else {
+#pragma unroll
+			for (int jj = 0; jj < 6; jj++)
+				tr[f][jj] = 0.0;
+		}
+	}
+	double yk[10], fv[10];
+	load10<double, double>(p.yacc + k * 60 + c * 10, yk);
+	load10<double, double>(p.f + k * 60 + c * 10, fv);
+	double s[4];
+#pragma unroll
+	for (int f = 0; f < 4; f++)
+		s[f] = p.sown64[u * 4 + f];
+	double cod[3][3];
+#pragma unroll
+	for (int a = 0; a < 3; a++)
+#pragma unroll
+		for (int b = 0; b < 3; b++)
+			cod[a][b] = p.geom[e * 10 + 3 * a + b];
+	const double coef = p.theta_dt / p.geom[e * 10 + 9];
+	const double *vv = p.vi + 3 * v;
+	double uk[3];
+#pragma unroll
+	for (int q = 0; q < 3; q++)
+		uk[q] = vv[0] * cod[0][q] + vv[1] * cod[1][q] + vv[2] * cod[2][q];
+	double t[10];
+#pragma unroll
+	for (int i = 0; i < 10; i++) {
+		double acc = 0.0;
+#pragma unroll
+		for (int j = 0; j < 10; j++) {
+			const double vij = -(uk[0] * tb.D[0][i][j] + uk[1] * tb.D[1][i][j] + uk[2] * tb.D[2][i][j]);
+			acc += vij * yk[j];
+		}
+		t[i] = acc;
+	}
+#pragma unroll
+	for (int f = 0; f < 4; f++) {
+		const bool out = s[f] > 0.0;
+#pragma unroll
+		for (int ii = 0; ii < 6; ii++) {
+			double acc = 0.0;
+#pragma unroll
+			for (int jj = 0; jj < 6; jj++)
+				if (!SPARSE || (smask(ii) >> jj & 1))
+					acc += tb.S[ii][jj] * (out ? yk[f2n(f, jj)] : tr[f][jj]);
+			t[f2n(f, ii)] += acc * s[f];
+		}
+	}
+	float rr[10];
+#pragma unroll
+	for (int i = 0; i < 10; i++) {
+		double acc = 0.0;
+#pragma unroll
+		for (int j = 0; j < 10; j++)
+			acc += tb.Minv[i][j] * t[j];
+		rr[i] = (float)(fv[i] - yk[i] - coef * acc);
+	}
+	store10<float, float>(p.r + k * 60 + c * 10, rr);
+}
+
+int launch_kin_residual(const KinResidualParams &p, int sparse, cudaStream_t s)
+{
+	if (p.nitems <= 0)
+		return GDN_CUDA_OK;
+	const unsigned grid = (unsigned)((p.nitems + kSwItems - 1) / kSwItems);
+	if (sparse)
+		kin_residual_kernel<true><<<grid, kSwThreads, 0, s>>>(p);
+	else
+		kin_residual_kernel<false><<<grid, kSwThreads, 0, s>>>(p);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
 
 // x = a_y y + a_f f (the Crank-Nicolson transport result), then the
 // relaxation of dg_apply_relaxation (dg.c:109-147): w = sum_v x_v,
 // f <- omega f_eq(w) + (1 - omega) x.  A thread per (element, node).
-template <typename S, typename T, int NV>
-__global__ void kin_relax_kernel(KinRelaxParams<S> p)
+template <typename F, typename Y, typename T, int NV>
+__global__ void kin_relax_kernel(KinRelaxParams p)
 {
 	const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (t >= p.ne * 10)
 		return;
 	const long long e = t / 10;
 	const int i = (int)(t % 10);
+	F *f = reinterpret_cast<F *>(p.f);
+	const Y *yv = reinterpret_cast<const Y *>(p.y);
 	T x[NV][6], w[6];
 	long long base[NV];
 #pragma unroll
@@ -358,7 +610,7 @@ __global__ void kin_relax_kernel(KinRelaxParams<S> p)
 #pragma unroll
 		for (int c = 0; c < 6; c++) {
 			const long long o = base[v] + c * 10;
-			const T xv = (T)p.a_y * (T)Store<S>::load(p.y + o) + (T)p.a_f * (T)Store<S>::load(p.f + o);
+			const T xv = (T)p.a_y * (T)Store<Y>::load(yv + o) + (T)p.a_f * (T)Store<F>::load(f + o);
 			x[v][c] = xv;
 			w[c] += xv;
 		}
@@ -372,24 +624,24 @@ __global__ void kin_relax_kernel(KinRelaxParams<S> p)
 #pragma unroll
 		for (int c = 0; c < 6; c++) {
 			const T feq = w[c] * inv_nv + fc * Aw[c];
-			Store<S>::store(p.f + base[v] + c * 10, om * feq + om1 * x[v][c]);
+			Store<F>::store(f + base[v] + c * 10, om * feq + om1 * x[v][c]);
 		}
 	}
 }
 
-template <typename S>
-int launch_kin_relax(const KinRelaxParams<S> &p, cudaStream_t s)
+template <typename F, typename Y, typename T>
+int launch_kin_relax(const KinRelaxParams &p, cudaStream_t s)
 {
-	typedef typename Store<S>::compute T;
 	const unsigned nblk = (unsigned)((p.ne * 10 + 255) / 256);
 	if (p.nv == 4)
-		kin_relax_kernel<S, T, 4><<<nblk, 256, 0, s>>>(p);
+		kin_relax_kernel<F, Y, T, 4><<<nblk, 256, 0, s>>>(p);
 	else
-		kin_relax_kernel<S, T, 6><<<nblk, 256, 0, s>>>(p);
+		kin_relax_kernel<F, Y, T, 6><<<nblk, 256, 0, s>>>(p);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_kin_relax<double>(const KinRelaxParams<double> &, cudaStream_t);
-template int launch_kin_relax<float>(const KinRelaxParams<float> &, cudaStream_t);
+template int launch_kin_relax<double, double, double>(const KinRelaxParams &, cudaStream_t);
+template int launch_kin_relax<float, float, float>(const KinRelaxParams &, cudaStream_t);
+template int launch_kin_relax<__nv_bfloat16, float, float>(const KinRelaxParams &, cudaStream_t);
 
 } // namespace gdn

@@ -128,3 +128,43 @@ def test_kinetic_step_host_equals_device_resident_steps():
     m = _vol_mask(s, mesh)
     s.close()
     assert np.array_equal(host[m], w7[m])
+
+
+def _variants(nb_v, n=6, jitter=0.15, mult=10, steps=10):
+    c, e = kuhn.kuhn_cube(n, jitter, seed=3)
+    mesh = capi.mesh_build(c, e)
+    dt = mult * 0.3 * mesh.hmin()
+    out = {}
+    for name, prec, passes in [("fp64", capi.FP64, 1), ("fp32", capi.FP32, 1), ("ref1", capi.FP32_REFINE, 1),
+                               ("ref2", capi.FP32_REFINE, 2), ("bf16", capi.BF16_STORE, 1)]:
+        s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, nb_v=nb_v, precision=prec,
+                        refine_passes=passes)
+        wn, t, _ = s.solve(steps)
+        out[name] = (wn, s.error_l2())
+        s.close()
+    return out
+
+
+@pytest.mark.parametrize("nb_v", [4, 6])
+def test_kinetic_fp32_refinement_recovers_fp64(nb_v):
+    """FP32 sweeps plus FP64-residual refinement: each pass multiplies the
+    distance to the FP64 solve by ~1e-6 (FP32 sweeps alone: ~1e-6)."""
+    out = _variants(nb_v)
+    ref = out["fp64"][0]
+    rel = {k: np.linalg.norm(v[0] - ref) / np.linalg.norm(ref) for k, v in out.items()}
+    assert 1e-8 < rel["fp32"] < 1e-5, rel
+    assert rel["ref1"] <= 1e-11, rel
+    assert rel["ref2"] <= 1e-13, rel
+    assert rel["ref2"] < rel["ref1"] < rel["fp32"]
+    # the analytic error of the refined runs is the FP64 one
+    assert abs(out["ref1"][1] - out["fp64"][1]) <= 1e-9 * out["fp64"][1]
+
+
+def test_kinetic_bf16_storage_error_is_bounded():
+    """BF16 distributions with FP32 arithmetic: the state stays within a few
+    1e-3 of the FP64 run on a coarse mesh (BF16 keeps 8 significant bits)."""
+    out = _variants(4)
+    ref = out["fp64"][0]
+    rel = np.linalg.norm(out["bf16"][0] - ref) / np.linalg.norm(ref)
+    assert 1e-4 < rel < 2e-2, rel
+    assert abs(out["bf16"][1] - out["fp64"][1]) <= 0.1 * out["fp64"][1]
