@@ -18,7 +18,7 @@ int launch_kin_setup(const int *face2elem, long long nf, const double *geom, con
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
 					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *rcoef,
-					  int4 *rnb, int4 *rpm, GT *rs, int *bad, cudaStream_t s);
+					  int4 *rnb, int4 *rpm, GT *rs, double4 *ru64, double4 *rs64, int *bad, cudaStream_t s);
 }
 
 using namespace gdn;
@@ -102,7 +102,8 @@ struct gdn_cuda_handle {
 	void *rs = nullptr; // [k][4] own-side v.vn
 	int4 *rnb = nullptr, *rpm = nullptr; // [k] inflow neighbour items, permutations
 	double *bt = nullptr; // [bf][v][6][6] boundary f_eq at t + dt/2
-	double *sown64 = nullptr; // [e * nv + v][4] v.vn in FP64 (refinement residual)
+	double *sown64 = nullptr; // [e * nv + v][4] v.vn in FP64
+	double4 *ru64 = nullptr, *rs64 = nullptr; // FP32_REFINE: [k] (u, theta dt / det), v.vn in FP64
 	double *yacc = nullptr; // FP32_REFINE: FP64 solution of the transport solve
 	float *rhs = nullptr; // FP32_REFINE: residual, right-hand side of the corrections
 	int refine_passes = 1;
@@ -506,6 +507,12 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->f), 60 * nu));
 		else
 			GDN_TRY(dalloc(h, reinterpret_cast<__nv_bfloat16 **>(&h->f), 60 * nu));
+		if (h->precision == GDN_CUDA_FP32_REFINE) {
+			GDN_TRY(dalloc(h, &h->yacc, 60 * nu));
+			GDN_TRY(dalloc(h, &h->rhs, 60 * nu));
+			GDN_TRY(dalloc(h, &h->ru64, nu));
+			GDN_TRY(dalloc(h, &h->rs64, nu));
+		}
 		if (fp64) {
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->G), 100 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->rs), 4 * nu));
@@ -513,7 +520,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->y), 60 * nu));
 			GDN_TRY(launch_kin_blocks<double>(h->geom64, h->sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
 											  h->theta * h->dt, as<double>(h->G), as<double>(h->rcoef), h->rnb,
-											  h->rpm, as<double>(h->rs), h->flag, s));
+											  h->rpm, as<double>(h->rs), h->ru64, h->rs64, h->flag, s));
 		} else {
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->G), 100 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->rs), 4 * nu));
@@ -521,11 +528,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->y), 60 * nu));
 			GDN_TRY(launch_kin_blocks<float>(h->geom64, h->sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
 											 h->theta * h->dt, as<float>(h->G), as<float>(h->rcoef), h->rnb, h->rpm,
-											 as<float>(h->rs), h->flag, s));
-		}
-		if (h->precision == GDN_CUDA_FP32_REFINE) {
-			GDN_TRY(dalloc(h, &h->yacc, 60 * nu));
-			GDN_TRY(dalloc(h, &h->rhs, 60 * nu));
+											 as<float>(h->rs), h->ru64, h->rs64, h->flag, s));
 		}
 		h->launches += 2;
 		GDN_CUDA_TRY(cudaMemcpyAsync(&bad, h->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -755,12 +758,9 @@ static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 		q.rnb = h->rnb;
 		q.rpm = h->rpm;
 		q.items = h->items;
-		q.sown64 = h->sown64;
-		q.geom = h->geom64;
+		q.ru64 = h->ru64;
+		q.rs64 = h->rs64;
 		q.bt = h->bt;
-		q.theta_dt = h->theta * h->dt;
-		for (int i = 0; i < 3 * NV_MAX; i++)
-			q.vi[i] = h->km.vi[i];
 		q.nv = h->nv;
 		q.nitems = h->ne * h->nv;
 		for (int pass = 0; pass < h->refine_passes; pass++) {

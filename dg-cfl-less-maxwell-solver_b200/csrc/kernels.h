@@ -76,11 +76,9 @@ struct KinResidualParams {
 	float *r;
 	const int4 *rnb, *rpm;
 	const int *items;
-	const double *sown64; // [e * nv + v][4]
-	const double *geom; // [e][10] FP64
+	const double4 *ru64; // [k] u_0, u_1, u_2 (u_q = v . codtau[:, q]), theta dt / det
+	const double4 *rs64; // [k] own-side v.vn per face
 	const double *bt;
-	double theta_dt;
-	double vi[3 * NV_MAX];
 	int nv;
 	long long nitems;
 };

@@ -80,7 +80,8 @@ __global__ void kin_mask_kernel(const double *__restrict__ sown64, const int *__
 template <typename GT>
 __global__ void kin_blocks_kernel(const double *__restrict__ geom, const double *__restrict__ sown64,
 								  const int *__restrict__ pos, long long ne, KinModel km, double theta_dt,
-								  GT *__restrict__ G, GT *__restrict__ rcoef, int *__restrict__ bad)
+								  GT *__restrict__ G, GT *__restrict__ rcoef, double4 *__restrict__ ru64,
+								  double4 *__restrict__ rs64, int *__restrict__ bad)
 {
 	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (u >= ne * km.nv)
@@ -154,6 +155,10 @@ __global__ void kin_blocks_kernel(const double *__restrict__ geom, const double 
 		for (int j = 0; j < 10; j++)
 			Gk[i * 10 + j] = (GT)a[i][10 + j];
 	rcoef[k] = (GT)c;
+	if (ru64) {
+		ru64[k] = make_double4(uk[0], uk[1], uk[2], c);
+		rs64[k] = make_double4(sown64[u * 4], sown64[u * 4 + 1], sown64[u * 4 + 2], sown64[u * 4 + 3]);
+	}
 }
 
 // per-item records of the sweep
@@ -201,11 +206,11 @@ int launch_kin_setup(const int *face2elem, long long nf, const double *geom, con
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
 					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *rcoef,
-					  int4 *rnb, int4 *rpm, GT *rs, int *bad, cudaStream_t s)
+					  int4 *rnb, int4 *rpm, GT *rs, double4 *ru64, double4 *rs64, int *bad, cudaStream_t s)
 {
 	const long long nu = ne * km.nv;
 	kin_blocks_kernel<GT><<<(unsigned)((nu + 127) / 128), 128, 0, s>>>(geom, sown64, pos, ne, km, theta_dt, G, rcoef,
-																	   bad);
+																	   ru64, rs64, bad);
 	GDN_CUDA_TRY(cudaGetLastError());
 	kin_records_kernel<GT><<<(unsigned)((nu + 255) / 256), 256, 0, s>>>(items, pos, sown64, nb, perm, nu, km.nv, rnb,
 																		rpm, rs);
@@ -216,10 +221,10 @@ template int launch_kin_setup<double>(const int *, long long, const double *, co
 									  const KinModel &, double *, unsigned char *, cudaStream_t);
 template int launch_kin_blocks<double>(const double *, const double *, const int *, const int *, const int *,
 									   const int *, long long, const KinModel &, double, double *, double *, int4 *,
-									   int4 *, double *, int *, cudaStream_t);
+									   int4 *, double *, double4 *, double4 *, int *, cudaStream_t);
 template int launch_kin_blocks<float>(const double *, const double *, const int *, const int *, const int *,
 									  const int *, long long, const KinModel &, double, float *, float *, int4 *,
-									  int4 *, float *, int *, cudaStream_t);
+									  int4 *, float *, double4 *, double4 *, int *, cudaStream_t);
 
 // f_eq of the analytic data at every boundary face node for every velocity,
 // at t + dt/2 (relaxation.c:99, dg_update_boundary with use_feq), formed from
@@ -321,7 +326,9 @@ __device__ __forceinline__ void store10(S *p, const T v[10])
 //   t = sum_inflow s E_f S tr_f,  r = f - coef Minv t,  y = G r.
 // G of the 32 items is staged by cp.async into shared memory while the
 // traces are in flight; its per-item stride (100 floats / 102 doubles) keeps
-// the 16-byte row reads conflict-free.
+// the 16-byte row reads conflict-free.  Levels are launched with programmatic
+// stream serialization: level l + 1 stages G, records and f while level l
+// runs, and waits (griddepcontrol.wait) only before its trace loads.
 constexpr int kSwItems = 32;
 constexpr int kSwThreads = 6 * 32;
 
@@ -337,6 +344,10 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 {
 	typedef SweepG<T> SG;
 	__shared__ __align__(16) T gsh[kSwItems * SG::stride];
+	// Programmatic dependent launch: the next level's CTAs may start now and
+	// run their prologue (everything below up to griddepcontrol.wait reads
+	// only data that no sweep level writes).
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
 	const long long k0 = (long long)p.item_begin + (long long)blockIdx.x * kSwItems;
 	const long long rem = (long long)p.item_end - k0;
@@ -352,14 +363,33 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 	}
 	const Tables<T> &tb = tab<T>();
 	const bool act = lane < nloc;
-	const long long k = k0 + lane;
-	T r[10];
-	if (act) {
-		const int4 nb4 = p.rnb[k];
-		const int4 pm4 = p.rpm[k];
-		const int nbk[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
-		const int pmk[4] = {pm4.x, pm4.y, pm4.z, pm4.w};
+	const long long k = k0 + (act ? lane : 0);
+	// prologue: this item's records, right-hand side and FP64 accumulator
+	const int4 nb4 = p.rnb[k];
+	const int4 pm4 = p.rpm[k];
+	const int nbk[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+	const int pmk[4] = {pm4.x, pm4.y, pm4.z, pm4.w};
+	T fv[10];
+	load10<F, T>(reinterpret_cast<const F *>(p.f) + k * 60 + c * 10, fv);
+	double ya[ACC == 2 ? 10 : 1];
+	if (ACC == 2)
+		load10<double, double>(p.yacc + k * 60 + c * 10, ya);
+	const T coef = reinterpret_cast<const T *>(p.rcoef)[k];
+	T s[4];
+	{
 		const T *rs = reinterpret_cast<const T *>(p.rs) + k * 4;
+#pragma unroll
+		for (int f = 0; f < 4; f++)
+			s[f] = rs[f];
+	}
+	int v = 0;
+	if (BD)
+		v = p.items[k] % p.nv;
+	// the upwind items of earlier levels are complete once the previous
+	// level's grid is
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	T r[10];
+	{
 		T tr[4][6];
 #pragma unroll
 		for (int f = 0; f < 4; f++) {
@@ -370,7 +400,6 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 				for (int jj = 0; jj < 6; jj++)
 					tr[f][jj] = (T)Store<Y>::load(yn + ((pmk[f] >> (4 * jj)) & 15));
 			} else if (BD && nbv != INT_MIN) {
-				const int v = p.items[k] % p.nv;
 				const double *b = p.bt + (((long long)(-nbv - 1) * p.nv + v) * 6 + c) * 6;
 #pragma unroll
 				for (int jj = 0; jj < 6; jj++)
@@ -381,13 +410,6 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 					tr[f][jj] = T(0);
 			}
 		}
-		T fv[10];
-		load10<F, T>(reinterpret_cast<const F *>(p.f) + k * 60 + c * 10, fv);
-		const T coef = reinterpret_cast<const T *>(p.rcoef)[k];
-		T s[4];
-#pragma unroll
-		for (int f = 0; f < 4; f++)
-			s[f] = rs[f];
 		// t_i = sum over the faces through node i of s_f (S tr_f)_ii
 		T t[10];
 #pragma unroll
@@ -434,11 +456,13 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 		}
 	}
 	store10<Y, T>(reinterpret_cast<Y *>(p.y) + k * 60 + c * 10, y);
-	if (ACC) {
-		double *ya = p.yacc + k * 60 + c * 10;
+	if (ACC == 1) {
+		store10<double, T>(p.yacc + k * 60 + c * 10, y);
+	} else if (ACC == 2) {
 #pragma unroll
 		for (int i = 0; i < 10; i++)
-			ya[i] = ACC == 1 ? (double)y[i] : ya[i] + (double)y[i];
+			ya[i] += (double)y[i];
+		store10<double, double>(p.yacc + k * 60 + c * 10, ya);
 	}
 }
 
@@ -448,8 +472,17 @@ int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cu
 	const long long n = (long long)p.item_end - p.item_begin;
 	if (n <= 0)
 		return GDN_CUDA_OK;
-	const unsigned grid = (unsigned)((n + kSwItems - 1) / kSwItems);
-#define GDN_SWEEP(A, B, SP) kin_sweep_kernel<F, Y, T, A, B, SP><<<grid, kSwThreads, 0, s>>>(p)
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)((n + kSwItems - 1) / kSwItems));
+	cfg.blockDim = dim3(kSwThreads);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = s;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+#define GDN_SWEEP(A, B, SP) GDN_CUDA_TRY(cudaLaunchKernelEx(&cfg, kin_sweep_kernel<F, Y, T, A, B, SP>, p))
 	if (acc == 0 && bdata) {
 		if (sparse)
 			GDN_SWEEP(0, true, true);
@@ -481,8 +514,8 @@ template int launch_kin_sweep<double, float, float>(const KinSweepParams &, int,
 // only reads y), same thread layout as the sweep:
 //   r = f - y - coef Minv (V y + sum_outflow s E S E^T y + sum_inflow s E S tr)
 // with V_ij = -(u . D_ij), u_k = v . codtau[:, k], tr the upwind neighbour's
-// y or the boundary f_eq.  This is f - b - M1 y with M1 exactly as the
-// blocks kernel builds it, in FP64 from the FP64 geometry and v.vn.
+// y or the boundary f_eq.  This is f - b - M1 y with M1 as the blocks kernel
+// builds it, from the FP64 u, theta dt / det and v.vn it records per item.
 template <bool SPARSE>
 __global__ void __launch_bounds__(kSwThreads) kin_residual_kernel(KinResidualParams p)
 {
@@ -491,9 +524,6 @@ __global__ void __launch_bounds__(kSwThreads) kin_residual_kernel(KinResidualPar
 	if (k >= p.nitems)
 		return;
 	const Tables<double> &tb = c_tab_d;
-	const long long u = p.items[k];
-	const long long e = u / p.nv;
-	const int v = (int)(u % p.nv);
 	const int4 nb4 = p.rnb[k];
 	const int4 pm4 = p.rpm[k];
 	const int nbk[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
@@ -508,6 +538,7 @@ __global__ void __launch_bounds__(kSwThreads) kin_residual_kernel(KinResidualPar
 			for (int jj = 0; jj < 6; jj++)
 				tr[f][jj] = yn[(pmk[f] >> (4 * jj)) & 15];
 		} else if (nbv != INT_MIN) {
+			const int v = p.items[k] % p.nv;
 			const double *b = p.bt + (((long long)(-nbv - 1) * p.nv + v) * 6 + c) * 6;
 #pragma unroll
 			for (int jj = 0; jj < 6; jj++)
@@ -521,32 +552,24 @@ __global__ void __launch_bounds__(kSwThreads) kin_residual_kernel(KinResidualPar
 	double yk[10], fv[10];
 	load10<double, double>(p.yacc + k * 60 + c * 10, yk);
 	load10<double, double>(p.f + k * 60 + c * 10, fv);
-	double s[4];
-#pragma unroll
-	for (int f = 0; f < 4; f++)
-		s[f] = p.sown64[u * 4 + f];
-	double cod[3][3];
-#pragma unroll
-	for (int a = 0; a < 3; a++)
-#pragma unroll
-		for (int b = 0; b < 3; b++)
-			cod[a][b] = p.geom[e * 10 + 3 * a + b];
-	const double coef = p.theta_dt / p.geom[e * 10 + 9];
-	const double *vv = p.vi + 3 * v;
-	double uk[3];
-#pragma unroll
-	for (int q = 0; q < 3; q++)
-		uk[q] = vv[0] * cod[0][q] + vv[1] * cod[1][q] + vv[2] * cod[2][q];
+	const double4 ru = p.ru64[k]; // u_0, u_1, u_2, theta dt / det
+	const double4 s4 = p.rs64[k];
+	const double s[4] = {s4.x, s4.y, s4.z, s4.w};
+	// V y = -(u_0 D_0 y + u_1 D_1 y + u_2 D_2 y)
 	double t[10];
 #pragma unroll
 	for (int i = 0; i < 10; i++) {
-		double acc = 0.0;
+		double g[3];
 #pragma unroll
-		for (int j = 0; j < 10; j++) {
-			const double vij = -(uk[0] * tb.D[0][i][j] + uk[1] * tb.D[1][i][j] + uk[2] * tb.D[2][i][j]);
-			acc += vij * yk[j];
+		for (int q = 0; q < 3; q++) {
+			double acc = 0.0;
+#pragma unroll
+			for (int j = 0; j < 10; j++)
+				if (!SPARSE || (dmask(q, i) >> j & 1))
+					acc += tb.D[q][i][j] * yk[j];
+			g[q] = acc;
 		}
-		t[i] = acc;
+		t[i] = -(ru.x * g[0] + ru.y * g[1] + ru.z * g[2]);
 	}
 #pragma unroll
 	for (int f = 0; f < 4; f++) {
@@ -568,7 +591,7 @@ __global__ void __launch_bounds__(kSwThreads) kin_residual_kernel(KinResidualPar
 #pragma unroll
 		for (int j = 0; j < 10; j++)
 			acc += tb.Minv[i][j] * t[j];
-		rr[i] = (float)(fv[i] - yk[i] - coef * acc);
+		rr[i] = (float)(fv[i] - yk[i] - ru.w * acc);
 	}
 	store10<float, float>(p.r + k * 60 + c * 10, rr);
 }
