@@ -59,6 +59,11 @@ class Model(C.Structure):
                 ("omega", C.c_double), ("vi", C.POINTER(C.c_double)), ("theta", C.c_double)]
 
 
+class Instance(C.Structure):
+    _fields_ = [("mesh", C.POINTER(Mesh)), ("model", C.POINTER(Model)), ("data", C.POINTER(Data)),
+                ("dt", C.c_double)]
+
+
 class Config(C.Structure):
     _fields_ = [("precision", C.c_int), ("refine_passes", C.c_int), ("elems_per_cta", C.c_int),
                 ("use_graph", C.c_int), ("device", C.c_int)]
@@ -69,7 +74,8 @@ EXPORTS = [
     "gdn_cuda_detach", "gdn_cuda_solve", "gdn_cuda_init", "gdn_cuda_advance",
     "gdn_cuda_set_state", "gdn_cuda_get_state", "gdn_cuda_step_host", "gdn_cuda_error_l2",
     "gdn_cuda_get_time", "gdn_cuda_state_size", "gdn_cuda_num_levels", "gdn_cuda_launch_count",
-    "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc",
+    "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc", "gdn_cuda_attach_batch",
+    "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_tile",
 ]
 
 _lib = None
@@ -104,6 +110,13 @@ def lib():
     L.gdn_cuda_stream.argtypes = [vp, C.POINTER(vp)]
     L.gdn_cuda_error_l2_noalloc.argtypes = [vp, vp, vp, C.c_longlong, dp, C.POINTER(Data),
                                             C.c_double, vp, dp]
+    L.gdn_cuda_attach_batch.argtypes = [C.POINTER(Instance), C.c_int, C.POINTER(Tables), C.POINTER(Config),
+                                        C.POINTER(vp)]
+    L.gdn_cuda_error_l2_batch.argtypes = [vp, dp]
+    L.gdn_cuda_num_instances.argtypes = [vp, ip]
+    L.gdn_cuda_rk3_tile.argtypes = [vp, ip]
+    L.gdn_cuda_instance_info.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                         C.POINTER(C.c_longlong)]
     _lib = L
     return L
 
@@ -229,26 +242,32 @@ class Solver:
                  precision=FP64, nb_v=4, tables: Tables = None, device=0, use_graph=1,
                  refine_passes=1, theta=0.5, elems_per_cta=0):
         self.L = lib()
+        self.h = C.c_void_p()
         self.mesh = mesh
         self.scheme = scheme
         self.tables = tables if tables is not None else t10_tables()
         self.data = data if data is not None else plane_data()
+        model = self._model(scheme, nb_v, theta)
+        cfg = Config(precision, refine_passes, elems_per_cta, use_graph, device)
+        check(self.L.gdn_cuda_attach(C.byref(mesh.struct), C.byref(self.tables), C.byref(model),
+                                     C.byref(self.data), C.byref(cfg), float(dt), C.byref(self.h)))
+        self.dt = float(dt)
+
+    def _model(self, scheme, nb_v, theta):
+        """The gdn_model descriptor of the scheme (vi kept alive on self)."""
         if scheme == SCHEME_RK3:
             self._vi = np.zeros(3, np.float64)
-            model = Model(SCHEME_RK3, 6, 0, 1.0, 0.0, _dp(self._vi), 0.5)
             self.m = 6
+            model = Model(SCHEME_RK3, 6, 0, 1.0, 0.0, _dp(self._vi), 0.5)
         else:
             lam = D3Q4_LAMBDA if nb_v == 4 else D3Q6_LAMBDA
             base = D3Q4_VI if nb_v == 4 else D3Q6_VI
             self._vi = np.ascontiguousarray((base * lam).ravel())
-            model = Model(SCHEME_KINETIC, 6, nb_v, lam, RELAX_OMEGA, _dp(self._vi), theta)
             self.m = 6 * nb_v
+            model = Model(SCHEME_KINETIC, 6, nb_v, lam, RELAX_OMEGA, _dp(self._vi), theta)
         self.nb_v = nb_v
-        cfg = Config(precision, refine_passes, elems_per_cta, use_graph, device)
-        self.h = C.c_void_p()
-        check(self.L.gdn_cuda_attach(C.byref(mesh.struct), C.byref(self.tables), C.byref(model),
-                                     C.byref(self.data), C.byref(cfg), float(dt), C.byref(self.h)))
-        self.dt = float(dt)
+        self._model_struct = model
+        return model
 
     @property
     def wlen(self) -> int:
@@ -299,6 +318,12 @@ class Solver:
         return n.value
 
     @property
+    def rk3_tile(self) -> int:
+        n = C.c_int()
+        check(self.L.gdn_cuda_rk3_tile(self.h, C.byref(n)))
+        return n.value
+
+    @property
     def launches(self) -> int:
         n = C.c_longlong()
         check(self.L.gdn_cuda_launch_count(self.h, C.byref(n)))
@@ -320,3 +345,55 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class BatchSolver(Solver):
+    """A batch of independent solves of one scheme in one handle
+    (gdn_cuda_attach_batch): every stage / step launch covers all instances;
+    each instance keeps its own mesh, data and dt."""
+
+    def __init__(self, meshes, datas, dts, scheme=SCHEME_RK3, precision=FP64, nb_v=4, tables: Tables = None,
+                 device=0, use_graph=1, refine_passes=1, theta=0.5, elems_per_cta=0):
+        self.L = lib()
+        self.h = C.c_void_p()
+        self.meshes = list(meshes)
+        self.datas = list(datas)
+        self.scheme = scheme
+        self.tables = tables if tables is not None else t10_tables()
+        model = self._model(scheme, nb_v, theta)
+        n = len(self.meshes)
+        self._inst = (Instance * n)()
+        for i in range(n):
+            self._inst[i].mesh = C.pointer(self.meshes[i].struct)
+            self._inst[i].model = C.pointer(model)
+            self._inst[i].data = C.pointer(self.datas[i])
+            self._inst[i].dt = float(dts[i])
+        cfg = Config(precision, refine_passes, elems_per_cta, use_graph, device)
+        check(self.L.gdn_cuda_attach_batch(self._inst, n, C.byref(self.tables), C.byref(cfg), C.byref(self.h)))
+        self.dts = [float(d) for d in dts]
+        self.dt = self.dts[0]
+
+    @property
+    def ninst(self) -> int:
+        n = C.c_int()
+        check(self.L.gdn_cuda_num_instances(self.h, C.byref(n)))
+        return n.value
+
+    def instance_info(self, i: int):
+        """(t, nbelems, offset, length) of instance i in the batch state."""
+        t, ne, off, ln = C.c_double(), C.c_longlong(), C.c_longlong(), C.c_longlong()
+        check(self.L.gdn_cuda_instance_info(self.h, int(i), C.byref(t), C.byref(ne), C.byref(off), C.byref(ln)))
+        return t.value, ne.value, off.value, ln.value
+
+    def split(self, wn: np.ndarray):
+        """The batch state as a list of per-instance reference-layout views."""
+        out = []
+        for i in range(self.ninst):
+            _, _, off, ln = self.instance_info(i)
+            out.append(wn[off:off + ln])
+        return out
+
+    def error_l2_batch(self) -> np.ndarray:
+        e = np.zeros(self.ninst, np.float64)
+        check(self.L.gdn_cuda_error_l2_batch(self.h, _dp(e)))
+        return e

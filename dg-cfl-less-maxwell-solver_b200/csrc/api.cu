@@ -5,7 +5,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "aux.h"
@@ -17,8 +20,9 @@ int launch_kin_setup(const int *face2elem, long long nf, const double *geom, con
 					 const KinModel &km, double *sown64, unsigned char *mask, cudaStream_t s);
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
-					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *rcoef,
-					  int4 *rnb, int4 *rpm, GT *rs, double4 *ru64, double4 *rs64, int *bad, cudaStream_t s);
+					  const int *perm, long long ne, const KinModel &km, double theta, const int *einst,
+					  const double *dt_tab, GT *G, GT *rcoef, int4 *rnb, int4 *rpm, GT *rs, double4 *ru64,
+					  double4 *rs64, int *bad, cudaStream_t s);
 }
 
 using namespace gdn;
@@ -64,11 +68,8 @@ struct gdn_cuda_handle {
 	cudaStream_t stream = nullptr;
 	int scheme = 0, precision = 0, nv = 0, use_graph = 1;
 	long long ne = 0, nf = 0, nbf = 0, nq = 0, neq = 0;
-	double dt = 0, theta = 0.5, omega = 0, lambda = 0;
-	Data data{};
+	double theta = 0.5, omega = 0, lambda = 0;
 	KinModel km{};
-	double t = 0; // current time (host copy, accumulated like the reference)
-	double t_bdof = 0; // RK3: time of the boundary data of the last stage
 	long long steps = 0;
 	long long launches = 0;
 	int ssize = 8; // bytes per stored state value
@@ -95,6 +96,7 @@ struct gdn_cuda_handle {
 	void *btrace = nullptr; // [nbf][6][6] boundary traces at the stage time
 	int cur = 0;
 	int rk3_variant = 0; // 0: field-per-warp tiles of 32, 1: element-per-thread tiles of 128
+	bool rk3_autotune = true; // pick the variant at attach by timing both
 	// kinetic, in sweep order (item k = position in the level-sorted list)
 	// f: FP64 (FP64, FP32_REFINE), FP32 or BF16; y: FP64 or FP32; G, rs,
 	// rcoef: FP64 (FP64) or FP32
@@ -111,9 +113,31 @@ struct gdn_cuda_handle {
 	int *pos = nullptr; // [e * nv + v] k
 	std::vector<int> level_off;
 	// device time and captured step loops
-	double *t_dev = nullptr;
+	double *t_dev = nullptr; // [ninst]
 	cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
 	long long graph_nodes[2] = {0, 0};
+	// batch of instances: concatenated meshes, per-instance dt / data / time.
+	// Offsets of instance i: elements e_off[i], boundary faces bf_off[i],
+	// reference-layout state w_off[i] (m * neq_i values each).
+	int ninst = 1;
+	std::vector<long long> e_off, bf_off, w_off, neq_i;
+	std::vector<Data> hdata;
+	std::vector<double> hdt, ht, ht_bdof; // host mirrors of dt, t, RK3 boundary-data time
+	int *einst = nullptr, *bfinst = nullptr; // nullptr for a single instance
+	Data *data_dev = nullptr;
+	double *dt_dev = nullptr;
+
+	Batch batch() const
+	{
+		Batch b;
+		b.einst = einst;
+		b.bfinst = bfinst;
+		b.data = data_dev;
+		b.dt = dt_dev;
+		b.t = t_dev;
+		b.ninst = ninst;
+		return b;
+	}
 };
 
 template <typename X>
@@ -400,12 +424,99 @@ static S *as(void *p)
 	return reinterpret_cast<S *>(p);
 }
 
+static const double RK_A[3] = {0., -5. / 9., -153. / 128.};
+static const double RK_B[3] = {1. / 3., 15. / 16., 8. / 15.};
+static const double RK_C[3] = {0., 1. / 3., 3. / 4.};
+
+// RK3 stage-kernel autotuner: times both work decompositions on the handle's
+// own buffers (contents are irrelevant to the timing; init / set_state
+// rewrite them) and keeps the faster one.  Decisions are cached per
+// (precision, floor(log2 ne)) for the life of the process.
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, int>, int> g_tune;
+
+template <typename T>
+static int autotune_rk3(gdn_cuda_handle *h)
+{
+	int bucket = 0;
+	while ((2LL << bucket) <= h->ne)
+		bucket++;
+	const std::pair<int, int> key(h->precision, bucket);
+	{
+		std::lock_guard<std::mutex> g(g_tune_mu);
+		auto it = g_tune.find(key);
+		if (it != g_tune.end()) {
+			h->rk3_variant = it->second;
+			return GDN_CUDA_OK;
+		}
+	}
+	Rk3Params<T> p;
+	p.w_in = as<T>(h->w[0]);
+	p.w_out = as<T>(h->w[1]);
+	p.k2 = as<T>(h->k2);
+	p.geom = reinterpret_cast<const T *>(h->geomT);
+	p.nb = h->nb;
+	p.perm = h->perm;
+	p.btrace = as<T>(h->btrace);
+	p.einst = h->einst;
+	p.dt_tab = h->dt_dev;
+	p.ne = h->ne;
+	p.dt = h->hdt[0];
+	p.A = RK_A[1];
+	p.B = RK_B[1];
+	p.stage0 = 0;
+	p.write_k2 = 1;
+	p.sparse = h->rk3_sparse;
+	cudaEvent_t ev[2];
+	GDN_CUDA_TRY(cudaEventCreate(&ev[0]));
+	GDN_CUDA_TRY(cudaEventCreate(&ev[1]));
+	float best = 0.f;
+	int pick = 0;
+	int rc = GDN_CUDA_OK;
+	for (int v = 0; v < 2 && rc == GDN_CUDA_OK; v++) {
+		float ms = 0.f;
+		for (int rep = 0; rep < 4 && rc == GDN_CUDA_OK; rep++) { // launch 0 warms up
+			if (rep == 1)
+				cudaEventRecord(ev[0], h->stream);
+			rc = v == 0 ? launch_rk3_stage<T>(p, h->stream) : launch_rk3_stage_ept<T>(p, h->stream);
+			h->launches++;
+		}
+		if (rc != GDN_CUDA_OK)
+			break;
+		cudaEventRecord(ev[1], h->stream);
+		cudaError_t e = cudaEventSynchronize(ev[1]);
+		if (e == cudaSuccess)
+			e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+		if (e != cudaSuccess)
+			rc = gdn_cuda_fail(e, "autotune_rk3", __FILE__, __LINE__);
+		if (v == 0 || ms < best) {
+			best = ms;
+			pick = v;
+		}
+	}
+	cudaEventDestroy(ev[0]);
+	cudaEventDestroy(ev[1]);
+	if (rc != GDN_CUDA_OK)
+		return rc;
+	h->rk3_variant = pick;
+	std::lock_guard<std::mutex> g(g_tune_mu);
+	g_tune[key] = pick;
+	return GDN_CUDA_OK;
+}
+
 static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cuda_tables *t,
 					   const gdn_cuda_model *mo)
 {
 	const long long ne = h->ne, nf = h->nf, nbf = h->nbf;
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
-	GDN_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+	// The kinetic step is a chain of small dependent sweep launches whose
+	// time is latency: its stream gets the highest priority, so that its CTAs
+	// are dispatched ahead of pending CTAs of throughput work (an RK3 batch)
+	// sharing the GPU.
+	int least = 0, greatest = 0;
+	GDN_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+	GDN_CUDA_TRY(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking,
+											  h->scheme == GDN_CUDA_SCHEME_KINETIC ? greatest : least));
 	if (!rk3_tables_standard_faces(t))
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: face2node differs from the P2 convention");
 	h->rk3_sparse = rk3_tables_sparse(t) ? 1 : 0;
@@ -425,9 +536,28 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 	h->nblk_err = 1184; // 8 x 148 SMs
 	GDN_TRY(dalloc(h, &h->partial, 6 * h->nblk_err));
 	GDN_TRY(dalloc(h, &h->result, 8));
-	GDN_TRY(dalloc(h, &h->t_dev, 1));
+	GDN_TRY(dalloc(h, &h->t_dev, h->ninst));
+	GDN_TRY(dalloc(h, &h->dt_dev, h->ninst));
+	GDN_TRY(dalloc(h, &h->data_dev, h->ninst));
 	GDN_CUDA_TRY(cudaMallocHost(&h->host_result, 8 * sizeof(double)));
 	cudaStream_t s = h->stream;
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->dt_dev, h->hdt.data(), h->ninst * sizeof(double), cudaMemcpyHostToDevice, s));
+	GDN_CUDA_TRY(
+		cudaMemcpyAsync(h->data_dev, h->hdata.data(), h->ninst * sizeof(Data), cudaMemcpyHostToDevice, s));
+	if (h->ninst > 1) {
+		std::vector<int> ei(ne), bi(nbf > 0 ? nbf : 1);
+		for (int i = 0; i < h->ninst; i++) {
+			for (long long e = h->e_off[i]; e < h->e_off[i + 1]; e++)
+				ei[e] = i;
+			for (long long b = h->bf_off[i]; b < h->bf_off[i + 1]; b++)
+				bi[b] = i;
+		}
+		GDN_TRY(dalloc(h, &h->einst, ne));
+		GDN_TRY(dalloc(h, &h->bfinst, bi.size()));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->einst, ei.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->bfinst, bi.data(), bi.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+		GDN_CUDA_TRY(cudaStreamSynchronize(s)); // the host vectors go out of scope
+	}
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->e2q, m->elem2qnode, 10 * ne * sizeof(int), cudaMemcpyHostToDevice, s));
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->node, m->node, 3 * h->nq * sizeof(double), cudaMemcpyHostToDevice, s));
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->nb, nb.data(), 4 * ne * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -477,6 +607,14 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->k2), 60 * ne));
 		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * ne * h->ssize, s));
 		GDN_TRY(dalloc(h, &h->staging, 6 * h->neq));
+		if (h->rk3_autotune) {
+			GDN_CUDA_TRY(cudaMemsetAsync(h->w[0], 0, 60 * ne * h->ssize, s));
+			GDN_CUDA_TRY(cudaMemsetAsync(h->btrace, 0, 36 * (nbf > 0 ? nbf : 1) * h->ssize, s));
+			if (fp64)
+				GDN_TRY(autotune_rk3<double>(h));
+			else
+				GDN_TRY(autotune_rk3<float>(h));
+		}
 	} else {
 		const int nv = h->nv;
 		h->neq = 10 * ne + 6 * nbf;
@@ -519,7 +657,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->rcoef), nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->y), 60 * nu));
 			GDN_TRY(launch_kin_blocks<double>(h->geom64, h->sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
-											  h->theta * h->dt, as<double>(h->G), as<double>(h->rcoef), h->rnb,
+											  h->theta, h->einst, h->dt_dev, as<double>(h->G), as<double>(h->rcoef), h->rnb,
 											  h->rpm, as<double>(h->rs), h->ru64, h->rs64, h->flag, s));
 		} else {
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->G), 100 * nu));
@@ -527,7 +665,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->rcoef), nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->y), 60 * nu));
 			GDN_TRY(launch_kin_blocks<float>(h->geom64, h->sown64, h->items, h->pos, h->nb, h->perm, ne, h->km,
-											 h->theta * h->dt, as<float>(h->G), as<float>(h->rcoef), h->rnb, h->rpm,
+											 h->theta, h->einst, h->dt_dev, as<float>(h->G), as<float>(h->rcoef), h->rnb, h->rpm,
 											 as<float>(h->rs), h->ru64, h->rs64, h->flag, s));
 		}
 		h->launches += 2;
@@ -540,28 +678,28 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 	return GDN_CUDA_OK;
 }
 
-extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
-							   const gdn_cuda_model *model, const gdn_cuda_data *data,
-							   const gdn_cuda_config *config, double dt, gdn_cuda_handle **out)
+static Data to_data(const gdn_cuda_data *d)
 {
-	if (!out)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: out is NULL");
-	*out = nullptr;
-	if (!tables || !model)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: tables or model missing");
-	GDN_TRY(validate_mesh(mesh));
-	GDN_TRY(validate_data(data));
-	if (!(dt > 0.0) || !std::isfinite(dt))
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: dt must be positive");
+	Data o;
+	o.kind = d->kind;
+	for (int c = 0; c < 3; c++) {
+		o.khat[c] = d->khat[c];
+		o.pol[c] = d->pol[c];
+	}
+	o.kmag = d->kmag;
+	o.amp = d->amp;
+	o.phase = d->phase;
+	return o;
+}
+
+static int validate_model(const gdn_cuda_model *model, const gdn_cuda_config &cfg)
+{
+	if (!model)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: model missing");
 	if (model->nb_w != 6)
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: only Maxwell (nb_w = 6) runs on the device");
 	if (model->scheme != GDN_CUDA_SCHEME_RK3 && model->scheme != GDN_CUDA_SCHEME_KINETIC)
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: unknown scheme");
-	gdn_cuda_config cfg = {GDN_CUDA_FP64, 1, 0, 1, 0};
-	if (config)
-		cfg = *config;
-	if (cfg.precision < GDN_CUDA_FP64 || cfg.precision > GDN_CUDA_BF16_STORE)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
 	if (model->scheme == GDN_CUDA_SCHEME_RK3 && cfg.precision > GDN_CUDA_FP32)
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: RK3 supports FP64 and FP32");
 	if (model->scheme == GDN_CUDA_SCHEME_KINETIC) {
@@ -572,6 +710,115 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 		if (cfg.precision == GDN_CUDA_FP32_REFINE && (cfg.refine_passes < 0 || cfg.refine_passes > 4))
 			return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: refine_passes must be in [0, 4]");
 	}
+	return GDN_CUDA_OK;
+}
+
+// instances of one batch share the scheme and, for the kinetic scheme, the
+// whole velocity model (one relaxation kernel serves them all)
+static bool same_model(const gdn_cuda_model *a, const gdn_cuda_model *b)
+{
+	if (a->scheme != b->scheme)
+		return false;
+	if (a->scheme == GDN_CUDA_SCHEME_RK3)
+		return true;
+	if (a->nb_v != b->nb_v || a->lambda != b->lambda || a->omega != b->omega || a->theta != b->theta)
+		return false;
+	for (int i = 0; i < 3 * a->nb_v; i++)
+		if (a->vi[i] != b->vi[i])
+			return false;
+	return true;
+}
+
+// host arrays of the concatenated mesh of a batch
+struct MeshCat {
+	std::vector<int> face2elem, fnode2enode, boundaryface, elem2qnode;
+	std::vector<double> node;
+	gdn_cuda_mesh m{};
+};
+
+static int concat_meshes(const gdn_cuda_instance *inst, int n, gdn_cuda_handle *h, MeshCat &mc)
+{
+	long long ne = 0, nf = 0, nbf = 0, nq = 0;
+	for (int i = 0; i < n; i++) {
+		ne += inst[i].mesh->nbelems;
+		nf += inst[i].mesh->nbfaces;
+		nbf += inst[i].mesh->nboundaryfaces;
+		nq += inst[i].mesh->nbqnodes;
+	}
+	if (ne > (1LL << 28) || nf > (1LL << 29) || nq > (1LL << 29))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: batch too large for 32-bit element / node indices");
+	mc.face2elem.resize(4 * nf);
+	mc.fnode2enode.resize(12 * nf);
+	mc.boundaryface.resize(nbf);
+	mc.elem2qnode.resize(10 * ne + 6 * nbf);
+	mc.node.resize(3 * nq);
+	long long e0 = 0, f0 = 0, b0 = 0, q0 = 0;
+	h->e_off.assign(1, 0);
+	h->bf_off.assign(1, 0);
+	for (int i = 0; i < n; i++) {
+		const gdn_cuda_mesh *m = inst[i].mesh;
+		for (long long F = 0; F < m->nbfaces; F++) {
+			const int *src = m->face2elem + 4 * F;
+			int *dst = mc.face2elem.data() + 4 * (f0 + F);
+			dst[0] = (int)(src[0] + e0);
+			dst[1] = src[1];
+			dst[2] = src[2] >= 0 ? (int)(src[2] + e0) : src[2];
+			dst[3] = src[3];
+		}
+		std::memcpy(mc.fnode2enode.data() + 12 * f0, m->fnode2enode, 12 * (size_t)m->nbfaces * sizeof(int));
+		for (long long b = 0; b < m->nboundaryfaces; b++)
+			mc.boundaryface[b0 + b] = (int)(m->boundaryface[b] + f0);
+		for (long long v = 0; v < 10LL * m->nbelems; v++)
+			mc.elem2qnode[10 * e0 + v] = (int)(m->elem2qnode[v] + q0);
+		for (long long v = 0; v < 6LL * m->nboundaryfaces; v++)
+			mc.elem2qnode[10 * ne + 6 * b0 + v] = (int)(m->elem2qnode[10LL * m->nbelems + v] + q0);
+		std::memcpy(mc.node.data() + 3 * q0, m->node, 3 * (size_t)m->nbqnodes * sizeof(double));
+		e0 += m->nbelems;
+		f0 += m->nbfaces;
+		b0 += m->nboundaryfaces;
+		q0 += m->nbqnodes;
+		h->e_off.push_back(e0);
+		h->bf_off.push_back(b0);
+	}
+	mc.m.nbelems = (int)ne;
+	mc.m.nbfaces = (int)nf;
+	mc.m.nboundaryfaces = (int)nbf;
+	mc.m.nbqnodes = (int)nq;
+	mc.m.face2elem = mc.face2elem.data();
+	mc.m.fnode2enode = mc.fnode2enode.data();
+	mc.m.boundaryface = mc.boundaryface.data();
+	mc.m.elem2qnode = mc.elem2qnode.data();
+	mc.m.node = mc.node.data();
+	return GDN_CUDA_OK;
+}
+
+static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tables *tables,
+						const gdn_cuda_config *config, gdn_cuda_handle **out)
+{
+	if (!out)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: out is NULL");
+	*out = nullptr;
+	if (!inst || n <= 0)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: no instances");
+	if (!tables)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: tables missing");
+	gdn_cuda_config cfg = {GDN_CUDA_FP64, 1, 0, 1, 0};
+	if (config)
+		cfg = *config;
+	if (cfg.precision < GDN_CUDA_FP64 || cfg.precision > GDN_CUDA_BF16_STORE)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
+	if (cfg.elems_per_cta != 0 && cfg.elems_per_cta != 32 && cfg.elems_per_cta != 128)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: elems_per_cta must be 0 (auto), 32 or 128");
+	for (int i = 0; i < n; i++) {
+		GDN_TRY(validate_mesh(inst[i].mesh));
+		GDN_TRY(validate_data(inst[i].data));
+		GDN_TRY(validate_model(inst[i].model, cfg));
+		if (!(inst[i].dt > 0.0) || !std::isfinite(inst[i].dt))
+			return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: dt must be positive");
+		if (!same_model(inst[0].model, inst[i].model))
+			return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED,
+								 "attach: the instances of a batch need one scheme and one kinetic model");
+	}
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
 		cudaGetLastError();
@@ -580,36 +827,28 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 	if (cfg.device < 0 || cfg.device >= ndev)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: bad device ordinal");
 
+	const gdn_cuda_model *model = inst[0].model;
 	gdn_cuda_handle *h = new gdn_cuda_handle();
 	h->device = cfg.device;
 	h->scheme = model->scheme;
 	h->precision = cfg.precision;
 	h->refine_passes = cfg.refine_passes;
 	h->use_graph = cfg.use_graph;
-	if (cfg.elems_per_cta != 0 && cfg.elems_per_cta != 32 && cfg.elems_per_cta != 128) {
-		delete h;
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: elems_per_cta must be 0 (auto), 32 or 128");
-	}
 	// RK3 stage kernel: 32-element tiles with a warp per field, or 128-element
-	// tiles with a thread per element
+	// tiles with a thread per element; 0 = timed at attach
 	h->rk3_variant = cfg.elems_per_cta == 128 ? 1 : 0;
-	h->ne = mesh->nbelems;
-	h->nf = mesh->nbfaces;
-	h->nbf = mesh->nboundaryfaces;
-	h->nq = mesh->nbqnodes;
-	h->dt = dt;
+	h->rk3_autotune = cfg.elems_per_cta == 0;
+	h->ninst = n;
+	for (int i = 0; i < n; i++) {
+		h->hdata.push_back(to_data(inst[i].data));
+		h->hdt.push_back(inst[i].dt);
+	}
+	h->ht.assign(n, 0.0);
+	h->ht_bdof.assign(n, 0.0);
 	h->theta = model->theta > 0 ? model->theta : 0.5;
 	h->omega = model->omega;
 	h->lambda = model->lambda;
 	h->ssize = cfg.precision == GDN_CUDA_FP64 ? 8 : 4;
-	h->data.kind = data->kind;
-	for (int c = 0; c < 3; c++) {
-		h->data.khat[c] = data->khat[c];
-		h->data.pol[c] = data->pol[c];
-	}
-	h->data.kmag = data->kmag;
-	h->data.amp = data->amp;
-	h->data.phase = data->phase;
 	if (h->scheme == GDN_CUDA_SCHEME_KINETIC) {
 		h->nv = model->nb_v;
 		h->km.nv = h->nv;
@@ -618,7 +857,30 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 		const double l2 = model->lambda * model->lambda;
 		h->km.feq_c = h->nv == 4 ? 1.0 / (4.0 * l2) : 1.0 / (2.0 * l2);
 	}
-	int rc = attach_impl(h, mesh, tables, model);
+	MeshCat mc;
+	const gdn_cuda_mesh *mesh = inst[0].mesh;
+	int rc = GDN_CUDA_OK;
+	if (n > 1) {
+		rc = concat_meshes(inst, n, h, mc);
+		mesh = &mc.m;
+	} else {
+		h->e_off = {0, mesh->nbelems};
+		h->bf_off = {0, mesh->nboundaryfaces};
+	}
+	if (rc == GDN_CUDA_OK) {
+		const long long m = h->scheme == GDN_CUDA_SCHEME_RK3 ? 6 : 6LL * h->nv;
+		h->w_off.assign(1, 0);
+		for (int i = 0; i < n; i++) {
+			const long long neq = 10 * (h->e_off[i + 1] - h->e_off[i]) + 6 * (h->bf_off[i + 1] - h->bf_off[i]);
+			h->neq_i.push_back(neq);
+			h->w_off.push_back(h->w_off.back() + m * neq);
+		}
+		h->ne = mesh->nbelems;
+		h->nf = mesh->nbfaces;
+		h->nbf = mesh->nboundaryfaces;
+		h->nq = mesh->nbqnodes;
+		rc = attach_impl(h, mesh, tables, model);
+	}
 	if (rc != GDN_CUDA_OK) {
 		std::string msg = g_last_error;
 		free_handle(h);
@@ -627,6 +889,24 @@ extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables 
 	}
 	*out = h;
 	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
+							   const gdn_cuda_model *model, const gdn_cuda_data *data,
+							   const gdn_cuda_config *config, double dt, gdn_cuda_handle **out)
+{
+	gdn_cuda_instance one;
+	one.mesh = mesh;
+	one.model = model;
+	one.data = data;
+	one.dt = dt;
+	return attach_batch(&one, 1, tables, config, out);
+}
+
+extern "C" int gdn_cuda_attach_batch(const gdn_cuda_instance *inst, int ninst, const gdn_cuda_tables *tables,
+									 const gdn_cuda_config *config, gdn_cuda_handle **out)
+{
+	return attach_batch(inst, ninst, tables, config, out);
 }
 
 extern "C" int gdn_cuda_detach(gdn_cuda_handle *h)
@@ -638,14 +918,12 @@ extern "C" int gdn_cuda_detach(gdn_cuda_handle *h)
 }
 
 // ------------------------------------------------------------ stepping --
-static const double RK_A[3] = {0., -5. / 9., -153. / 128.};
-static const double RK_B[3] = {1. / 3., 15. / 16., 8. / 15.};
-static const double RK_C[3] = {0., 1. / 3., 3. / 4.};
 
 // ---- enqueue one time step (no host bookkeeping; capturable) ----
 template <typename T>
 static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 {
+	const Batch bt = h->batch();
 	for (int i = 0; i < 3; i++) {
 		Rk3Params<T> p;
 		p.w_in = as<T>(h->w[cur]);
@@ -654,19 +932,18 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 		p.geom = reinterpret_cast<const T *>(h->geomT);
 		p.nb = h->nb;
 		p.perm = h->perm;
-		p.bxyz = h->bxyz;
 		p.btrace = as<T>(h->btrace);
-		p.data = h->data;
+		p.einst = h->einst;
+		p.dt_tab = h->dt_dev;
 		p.ne = h->ne;
-		p.dt = h->dt;
+		p.dt = h->hdt[0];
 		p.A = RK_A[i];
 		p.B = RK_B[i];
 		p.stage0 = i == 0;
 		p.write_k2 = i < 2;
 		p.sparse = h->rk3_sparse;
 		if (h->nbf > 0) {
-			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, h->data, h->t_dev, RK_C[i], h->dt, as<T>(h->btrace),
-											 h->stream));
+			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, bt, RK_C[i], as<T>(h->btrace), h->stream));
 			nlaunch++;
 		}
 		if (h->rk3_variant == 1)
@@ -676,7 +953,7 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 		nlaunch++;
 		cur = 1 - cur;
 	}
-	GDN_TRY(launch_advance_time(h->t_dev, h->dt, h->stream));
+	GDN_TRY(launch_advance_time(bt, h->stream));
 	nlaunch++;
 	return GDN_CUDA_OK;
 }
@@ -732,8 +1009,8 @@ static int kin_relax(gdn_cuda_handle *h, const void *y, long long &nlaunch)
 static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 {
 	if (h->nbf > 0) {
-		GDN_TRY(launch_kin_boundary_trace(h->bxyz, h->nbf, h->data, h->t_dev, h->dt, h->nv, h->km.vi, h->km.feq_c,
-										  h->bt, h->stream));
+		GDN_TRY(launch_kin_boundary_trace(h->bxyz, h->nbf, h->batch(), h->nv, h->km.vi, h->km.feq_c, h->bt,
+										  h->stream));
 		nlaunch++;
 	}
 	switch (h->precision) {
@@ -772,7 +1049,7 @@ static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 		break;
 	}
 	}
-	GDN_TRY(launch_advance_time(h->t_dev, h->dt, h->stream));
+	GDN_TRY(launch_advance_time(h->batch(), h->stream));
 	nlaunch++;
 	return GDN_CUDA_OK;
 }
@@ -792,11 +1069,13 @@ static int enqueue_steps(gdn_cuda_handle *h, int nsteps, int &cur, long long &nl
 	return GDN_CUDA_OK;
 }
 
-// host mirror of the device time, as the reference accumulates it
+// host mirror of the device times, as the reference accumulates them
 static void bookkeep_step(gdn_cuda_handle *h)
 {
-	h->t_bdof = h->t + RK_C[2] * h->dt;
-	h->t += h->dt;
+	for (int i = 0; i < h->ninst; i++) {
+		h->ht_bdof[i] = h->ht[i] + RK_C[2] * h->hdt[i];
+		h->ht[i] += h->hdt[i];
+	}
 	h->steps++;
 }
 
@@ -866,107 +1145,135 @@ static int kin_state_kind(const gdn_cuda_handle *h)
 	return 0;
 }
 
-// kinetic state <-> reference layout in the staging buffer
-static int kin_pack(gdn_cuda_handle *h, int to_ref)
+// kinetic state of instance i <-> its reference layout in the staging buffer
+static int kin_pack(gdn_cuda_handle *h, int i, int to_ref)
 {
 	const int sk = kin_state_kind(h);
+	const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
+	const int *pos = h->pos + e0 * h->nv;
+	double *st = h->staging + h->w_off[i];
+	const long long neq = h->neq_i[i];
 	if (sk == 0)
-		return launch_kin_pack<double>(as<double>(h->f), h->pos, h->ne, h->nv, h->neq, h->staging, to_ref, h->stream);
+		return launch_kin_pack<double>(as<double>(h->f), pos, ne, h->nv, neq, st, to_ref, h->stream);
 	if (sk == 1)
-		return launch_kin_pack<float>(as<float>(h->f), h->pos, h->ne, h->nv, h->neq, h->staging, to_ref, h->stream);
-	return launch_kin_pack<__nv_bfloat16>(as<__nv_bfloat16>(h->f), h->pos, h->ne, h->nv, h->neq, h->staging, to_ref,
-										  h->stream);
+		return launch_kin_pack<float>(as<float>(h->f), pos, ne, h->nv, neq, st, to_ref, h->stream);
+	return launch_kin_pack<__nv_bfloat16>(as<__nv_bfloat16>(h->f), pos, ne, h->nv, neq, st, to_ref, h->stream);
 }
 
+// dg_init_sol_macro (dg.c:32-59) of every instance with its own data
 extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
 {
 	if (!h)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "init: NULL handle");
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
 	cudaStream_t s = h->stream;
+	const int sk = h->scheme == GDN_CUDA_SCHEME_KINETIC ? kin_state_kind(h) : 0;
+	for (int i = 0; i < h->ninst; i++) {
+		const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
+		const int *e2q = h->e2q + 10 * e0;
+		const Data &d = h->hdata[i];
+		if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(launch_init_rk3<double>(e2q, h->node, ne, d, as<double>(h->w[0]) + 60 * e0, s));
+			else
+				GDN_TRY(launch_init_rk3<float>(e2q, h->node, ne, d, as<float>(h->w[0]) + 60 * e0, s));
+		} else {
+			const int *pos = h->pos + e0 * h->nv;
+			if (sk == 0)
+				GDN_TRY(launch_init_kin<double>(e2q, h->node, ne, d, h->km, pos, as<double>(h->f), s));
+			else if (sk == 1)
+				GDN_TRY(launch_init_kin<float>(e2q, h->node, ne, d, h->km, pos, as<float>(h->f), s));
+			else
+				GDN_TRY(launch_init_kin<__nv_bfloat16>(e2q, h->node, ne, d, h->km, pos, as<__nv_bfloat16>(h->f), s));
+		}
+		h->launches++;
+	}
 	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
 		h->cur = 0;
-		if (h->precision == GDN_CUDA_FP64)
-			GDN_TRY(launch_init_rk3<double>(h->e2q, h->node, h->ne, h->data, as<double>(h->w[0]), s));
-		else
-			GDN_TRY(launch_init_rk3<float>(h->e2q, h->node, h->ne, h->data, as<float>(h->w[0]), s));
 		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
-	} else {
-		const int sk = kin_state_kind(h);
-		if (sk == 0)
-			GDN_TRY(launch_init_kin<double>(h->e2q, h->node, h->ne, h->data, h->km, h->pos, as<double>(h->f), s));
-		else if (sk == 1)
-			GDN_TRY(launch_init_kin<float>(h->e2q, h->node, h->ne, h->data, h->km, h->pos, as<float>(h->f), s));
-		else
-			GDN_TRY(launch_init_kin<__nv_bfloat16>(h->e2q, h->node, h->ne, h->data, h->km, h->pos,
-												   as<__nv_bfloat16>(h->f), s));
 	}
+	GDN_TRY(launch_set_time(h->batch(), 0.0, s));
 	h->launches++;
-	GDN_TRY(launch_set_time(h->t_dev, 0.0, s));
-	h->launches++;
-	h->t = 0.0;
-	h->t_bdof = 0.0;
+	h->ht.assign(h->ninst, 0.0);
+	h->ht_bdof.assign(h->ninst, 0.0);
 	h->steps = 0;
 	return GDN_CUDA_OK;
 }
 
 // reference-layout state -> device (boundary dofs are not state on the
-// device: they are analytic data, re-derived when written back)
+// device: they are analytic data, re-derived when written back).  A batch
+// state is the concatenation of the instances' reference-layout vectors.
 extern "C" int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t)
 {
 	if (!h || !wn)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "set_state: bad arguments");
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
 	cudaStream_t s = h->stream;
-	const long long ne = h->ne;
 	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
 		h->cur = 0;
-		if (h->precision == GDN_CUDA_FP64) {
-			GDN_CUDA_TRY(cudaMemcpyAsync(h->w[0], wn, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
-		} else {
-			GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
-			GDN_TRY(launch_convert<float>(h->staging, as<float>(h->w[0]), 60 * ne, s));
+		for (int i = 0; i < h->ninst; i++) {
+			const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
+			const double *src = wn + h->w_off[i];
+			if (h->precision == GDN_CUDA_FP64) {
+				GDN_CUDA_TRY(cudaMemcpyAsync(as<double>(h->w[0]) + 60 * e0, src, 60 * ne * sizeof(double),
+											 cudaMemcpyHostToDevice, s));
+			} else {
+				double *st = h->staging + h->w_off[i];
+				GDN_CUDA_TRY(cudaMemcpyAsync(st, src, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
+				GDN_TRY(launch_convert<float>(st, as<float>(h->w[0]) + 60 * e0, 60 * ne, s));
+				h->launches++;
+			}
+		}
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
+	} else {
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, h->w_off.back() * sizeof(double), cudaMemcpyHostToDevice, s));
+		for (int i = 0; i < h->ninst; i++) {
+			GDN_TRY(kin_pack(h, i, 0));
 			h->launches++;
 		}
-		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * ne * h->ssize, s));
-	} else {
-		const long long wl = (long long)6 * h->nv * h->neq;
-		GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, wl * sizeof(double), cudaMemcpyHostToDevice, s));
-		GDN_TRY(kin_pack(h, 0));
-		h->launches++;
 	}
-	GDN_TRY(launch_set_time(h->t_dev, t, s));
+	GDN_TRY(launch_set_time(h->batch(), t, s));
 	h->launches++;
-	h->t = t;
-	h->t_bdof = t;
+	h->ht.assign(h->ninst, t);
+	h->ht_bdof.assign(h->ninst, t);
 	return GDN_CUDA_OK;
 }
 
 static int get_state_impl(gdn_cuda_handle *h, double *wn)
 {
 	cudaStream_t s = h->stream;
-	const long long ne = h->ne;
-	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
-		double *bd = h->staging + 60 * ne;
-		GDN_TRY(launch_boundary_dofs(h->bxyz, h->nbf, h->data, h->t_bdof, 0, h->km, h->neq, bd, s));
-		h->launches++;
-		if (h->precision == GDN_CUDA_FP64) {
-			GDN_CUDA_TRY(
-				cudaMemcpyAsync(wn, h->w[h->cur], 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
-		} else {
-			GDN_TRY(launch_widen(as<float>(h->w[h->cur]), h->staging, 60 * ne, s));
+	for (int i = 0; i < h->ninst; i++) {
+		const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
+		const long long b0 = h->bf_off[i], nbf = h->bf_off[i + 1] - b0;
+		const long long neq = h->neq_i[i];
+		double *st = h->staging + h->w_off[i];
+		double *dst = wn + h->w_off[i];
+		if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+			// boundary dofs at the time of the last stage's boundary data
+			GDN_TRY(launch_boundary_dofs(h->bxyz + 18 * b0, nbf, h->hdata[i], h->ht_bdof[i], 0, h->km, neq,
+										 st + 60 * ne, s));
 			h->launches++;
-			GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
+			if (h->precision == GDN_CUDA_FP64) {
+				GDN_CUDA_TRY(cudaMemcpyAsync(dst, as<double>(h->w[h->cur]) + 60 * e0, 60 * ne * sizeof(double),
+											 cudaMemcpyDeviceToHost, s));
+			} else {
+				GDN_TRY(launch_widen(as<float>(h->w[h->cur]) + 60 * e0, st, 60 * ne, s));
+				h->launches++;
+				GDN_CUDA_TRY(cudaMemcpyAsync(dst, st, 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
+			}
+			if (nbf > 0)
+				GDN_CUDA_TRY(cudaMemcpyAsync(dst + 60 * ne, st + 60 * ne, 36 * nbf * sizeof(double),
+											 cudaMemcpyDeviceToHost, s));
+		} else {
+			// boundary dofs after dg_update_boundary(simu, t) (relaxation.c:175)
+			GDN_TRY(launch_boundary_dofs(h->bxyz + 18 * b0, nbf, h->hdata[i], h->ht[i], 1, h->km, neq, st + 10 * ne,
+										 s));
+			GDN_TRY(kin_pack(h, i, 1));
+			h->launches += 2;
 		}
-		GDN_CUDA_TRY(cudaMemcpyAsync(wn + 60 * ne, bd, 36 * h->nbf * sizeof(double), cudaMemcpyDeviceToHost, s));
-	} else {
-		// boundary dofs after dg_update_boundary(simu, t) (relaxation.c:175)
-		GDN_TRY(launch_boundary_dofs(h->bxyz, h->nbf, h->data, h->t, 1, h->km, h->neq, h->staging + 10 * ne, s));
-		GDN_TRY(kin_pack(h, 1));
-		h->launches += 2;
-		GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, (long long)6 * h->nv * h->neq * sizeof(double),
-									 cudaMemcpyDeviceToHost, s));
 	}
+	if (h->scheme == GDN_CUDA_SCHEME_KINETIC)
+		GDN_CUDA_TRY(cudaMemcpyAsync(wn, h->staging, h->w_off.back() * sizeof(double), cudaMemcpyDeviceToHost, s));
 	GDN_CUDA_TRY(cudaStreamSynchronize(s));
 	return GDN_CUDA_OK;
 }
@@ -983,7 +1290,9 @@ extern "C" int gdn_cuda_step_host(gdn_cuda_handle *h, double *wn, int nsteps)
 {
 	if (!h || !wn || nsteps < 0)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "step_host: bad arguments");
-	GDN_TRY(gdn_cuda_set_state(h, wn, h->t));
+	if (h->ninst > 1)
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "step_host: one instance per handle");
+	GDN_TRY(gdn_cuda_set_state(h, wn, h->ht[0]));
 	GDN_TRY(advance_impl(h, nsteps));
 	return get_state_impl(h, wn);
 }
@@ -1000,9 +1309,39 @@ extern "C" int gdn_cuda_solve(gdn_cuda_handle *h, int itermax, double *wn, doubl
 	auto t1 = std::chrono::steady_clock::now();
 	GDN_TRY(get_state_impl(h, wn));
 	if (t)
-		*t = h->t;
+		*t = h->ht[0];
 	if (cpu_running_t)
 		*cpu_running_t = std::chrono::duration<double>(t1 - t0).count();
+	return GDN_CUDA_OK;
+}
+
+// simulation_error_l2 of instance i at its current time
+static int error_l2_impl(gdn_cuda_handle *h, int i, double *err)
+{
+	cudaStream_t s = h->stream;
+	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
+	const int sk = kin ? kin_state_kind(h) : (h->precision == GDN_CUDA_FP64 ? 0 : 1);
+	const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
+	const long long so = kin ? 0 : 60 * e0; // RK3 state offset; kinetic goes through pos
+	const int *pos = kin ? h->pos + e0 * h->nv : nullptr;
+	const int *e2q = h->e2q + 10 * e0;
+	const double *geom = h->geom64 + 10 * e0;
+	void *st = kin ? h->f : h->w[h->cur];
+	const double t = h->ht[i];
+	const Data &d = h->hdata[i];
+	if (sk == 0)
+		GDN_TRY(launch_error_l2<double>(as<double>(st) + so, kin, h->nv, pos, e2q, h->node, geom, ne, d, t,
+										h->partial, h->nblk_err, h->result, s));
+	else if (sk == 1)
+		GDN_TRY(launch_error_l2<float>(as<float>(st) + so, kin, h->nv, pos, e2q, h->node, geom, ne, d, t, h->partial,
+									   h->nblk_err, h->result, s));
+	else
+		GDN_TRY(launch_error_l2<__nv_bfloat16>(as<__nv_bfloat16>(st) + so, kin, h->nv, pos, e2q, h->node, geom, ne, d,
+											   t, h->partial, h->nblk_err, h->result, s));
+	h->launches += 2;
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->host_result, h->result, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
+	GDN_CUDA_TRY(cudaStreamSynchronize(s));
+	*err = h->host_result[0];
 	return GDN_CUDA_OK;
 }
 
@@ -1011,24 +1350,16 @@ extern "C" int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err)
 	if (!h || !err)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "error_l2: bad arguments");
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
-	cudaStream_t s = h->stream;
-	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
-	const void *st = kin ? h->f : h->w[h->cur];
-	const int sk = kin ? kin_state_kind(h) : (h->precision == GDN_CUDA_FP64 ? 0 : 1);
-	if (sk == 0)
-		GDN_TRY(launch_error_l2<double>(as<double>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q, h->node,
-										h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
-	else if (sk == 1)
-		GDN_TRY(launch_error_l2<float>(as<float>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q, h->node,
-									   h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err, h->result, s));
-	else
-		GDN_TRY(launch_error_l2<__nv_bfloat16>(as<__nv_bfloat16>(const_cast<void *>(st)), kin, h->nv, h->pos, h->e2q,
-											   h->node, h->geom64, h->ne, h->data, h->t, h->partial, h->nblk_err,
-											   h->result, s));
-	h->launches += 2;
-	GDN_CUDA_TRY(cudaMemcpyAsync(h->host_result, h->result, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
-	GDN_CUDA_TRY(cudaStreamSynchronize(s));
-	*err = h->host_result[0];
+	return error_l2_impl(h, 0, err);
+}
+
+extern "C" int gdn_cuda_error_l2_batch(gdn_cuda_handle *h, double *err)
+{
+	if (!h || !err)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "error_l2_batch: bad arguments");
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	for (int i = 0; i < h->ninst; i++)
+		GDN_TRY(error_l2_impl(h, i, err + i));
 	return GDN_CUDA_OK;
 }
 
@@ -1036,7 +1367,39 @@ extern "C" int gdn_cuda_get_time(gdn_cuda_handle *h, double *t)
 {
 	if (!h || !t)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "get_time: bad arguments");
-	*t = h->t;
+	*t = h->ht[0];
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_rk3_tile(gdn_cuda_handle *h, int *elems_per_cta)
+{
+	if (!h || !elems_per_cta)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "rk3_tile: bad arguments");
+	*elems_per_cta = h->scheme == GDN_CUDA_SCHEME_RK3 ? (h->rk3_variant == 1 ? 128 : 32) : 0;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_num_instances(gdn_cuda_handle *h, int *n)
+{
+	if (!h || !n)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "num_instances: bad arguments");
+	*n = h->ninst;
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_instance_info(gdn_cuda_handle *h, int i, double *t, long long *nbelems,
+									  long long *w_offset, long long *wlen)
+{
+	if (!h || i < 0 || i >= h->ninst)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "instance_info: bad arguments");
+	if (t)
+		*t = h->ht[i];
+	if (nbelems)
+		*nbelems = h->e_off[i + 1] - h->e_off[i];
+	if (w_offset)
+		*w_offset = h->w_off[i];
+	if (wlen)
+		*wlen = h->w_off[i + 1] - h->w_off[i];
 	return GDN_CUDA_OK;
 }
 
@@ -1044,7 +1407,7 @@ extern "C" int gdn_cuda_state_size(gdn_cuda_handle *h, long long *wlen)
 {
 	if (!h || !wlen)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "state_size: bad arguments");
-	*wlen = (h->scheme == GDN_CUDA_SCHEME_RK3 ? 6LL : 6LL * h->nv) * h->neq;
+	*wlen = h->w_off.back();
 	return GDN_CUDA_OK;
 }
 

@@ -180,60 +180,60 @@ __global__ void boundary_dofs_kernel(const double *__restrict__ bxyz, long long 
 
 // RK3 boundary traces at a stage time, in the stage kernels' precision:
 // out[(bf*6 + jj)*6 + c] = w_exact(x_{bf,jj}, t)_c  (dg_update_boundary,
-// dg.c:101-104, evaluated once per stage instead of inside the flux loop)
-// The stage time t + C_i dt is formed from the device copy of t with the
-// host's rounding (no fused multiply-add), so every stage sees the
-// reference's time bits.
+// dg.c:101-104, evaluated once per stage instead of inside the flux loop),
+// with the data, time and time step of the face's instance.  The stage time
+// t + C_i dt is formed from the device copy of t with the host's rounding (no
+// fused multiply-add), so every stage sees the reference's time bits.
 template <typename T>
-__global__ void boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Data d,
-									  const double *__restrict__ t_dev, double c_stage, double dt,
+__global__ void boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Batch b, double c_stage,
 									  T *__restrict__ out)
 {
 	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (u >= nbf * 6)
 		return;
-	const double t = __dadd_rn(*t_dev, __dmul_rn(c_stage, dt));
+	const int inst = b.bfinst ? b.bfinst[u / 6] : 0;
+	const double t = __dadd_rn(b.t[inst], __dmul_rn(c_stage, b.dt[inst]));
 	double x[3] = {bxyz[3 * u], bxyz[3 * u + 1], bxyz[3 * u + 2]}, we[6];
-	exact_w(d, x, t, we);
+	exact_w(b.data[inst], x, t, we);
 	for (int c = 0; c < 6; c++)
 		out[u * 6 + c] = (T)we[c];
 }
 
 template <typename T>
-int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double c_stage,
-						  double dt, T *out, cudaStream_t s)
+int launch_boundary_trace(const double *bxyz, long long nbf, const Batch &b, double c_stage, T *out, cudaStream_t s)
 {
 	if (nbf <= 0)
 		return GDN_CUDA_OK;
-	boundary_trace_kernel<T><<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, d, t_dev, c_stage, dt,
-																				out);
+	boundary_trace_kernel<T><<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, b, c_stage, out);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_boundary_trace<double>(const double *, long long, const Data &, const double *, double, double,
-										   double *, cudaStream_t);
-template int launch_boundary_trace<float>(const double *, long long, const Data &, const double *, double, double,
-										  float *, cudaStream_t);
+template int launch_boundary_trace<double>(const double *, long long, const Batch &, double, double *, cudaStream_t);
+template int launch_boundary_trace<float>(const double *, long long, const Batch &, double, float *, cudaStream_t);
 
-// device time: t = value, and t += dt (the reference's accumulation,
-// explicit.c:103 / relaxation.c:171)
-__global__ void set_time_kernel(double *t, double value)
+// device time of every instance: t = value, and t += dt (the reference's
+// accumulation, explicit.c:103 / relaxation.c:171)
+__global__ void set_time_kernel(Batch b, double value)
 {
-	*t = value;
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < b.ninst)
+		b.t[i] = value;
 }
-__global__ void advance_time_kernel(double *t, double dt)
+__global__ void advance_time_kernel(Batch b)
 {
-	*t = __dadd_rn(*t, dt);
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < b.ninst)
+		b.t[i] = __dadd_rn(b.t[i], b.dt[i]);
 }
-int launch_set_time(double *t, double value, cudaStream_t s)
+int launch_set_time(const Batch &b, double value, cudaStream_t s)
 {
-	set_time_kernel<<<1, 1, 0, s>>>(t, value);
+	set_time_kernel<<<(b.ninst + 127) / 128, 128, 0, s>>>(b, value);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-int launch_advance_time(double *t, double dt, cudaStream_t s)
+int launch_advance_time(const Batch &b, cudaStream_t s)
 {
-	advance_time_kernel<<<1, 1, 0, s>>>(t, dt);
+	advance_time_kernel<<<(b.ninst + 127) / 128, 128, 0, s>>>(b);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }

@@ -5,6 +5,19 @@
 
 namespace gdn {
 
+// A handle holds a batch of independent solves (one or more instances): their
+// meshes are concatenated (elements, faces, boundary faces and P2 nodes of
+// instance i follow those of instance i - 1), and each instance keeps its
+// own time step, analytic data and time.
+struct Batch {
+	const int *einst; // [ne] instance of each element (nullptr: one instance)
+	const int *bfinst; // [nbf] instance of each boundary face (nullptr: one instance)
+	const Data *data; // [ninst] analytic data
+	const double *dt; // [ninst] time step
+	double *t; // [ninst] device time
+	int ninst;
+};
+
 template <typename T>
 struct Rk3Params {
 	const T *w_in; // [ne][10][6] state read this stage
@@ -13,9 +26,9 @@ struct Rk3Params {
 	const T *geom; // [ne][10] codtau (row-major 3x3), det
 	const int *nb; // [ne][4] neighbour element, or -(boundary face + 1)
 	const int *perm; // [ne][4] neighbour local node of face node jj, 4 bits each
-	const double *bxyz; // [nbf][6][3] boundary face-node coordinates
 	const T *btrace; // [nbf][6][6] boundary data at t_stage (boundary_trace_kernel)
-	Data data;
+	const int *einst; // [ne] instance of each element, nullptr for one instance
+	const double *dt_tab; // [ninst] time step of each instance (used with einst)
 	long long ne;
 	double dt, A, B;
 	int stage0; // k2 = -dt dw (no k2 read)
@@ -35,10 +48,9 @@ int launch_rk3_stage_ept(const Rk3Params<T> &p, cudaStream_t s);
 template <typename T>
 int prepare_rk3_ept();
 template <typename T>
-int launch_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double c_stage,
-						  double dt, T *out, cudaStream_t s);
-int launch_set_time(double *t, double value, cudaStream_t s);
-int launch_advance_time(double *t, double dt, cudaStream_t s);
+int launch_boundary_trace(const double *bxyz, long long nbf, const Batch &b, double c_stage, T *out, cudaStream_t s);
+int launch_set_time(const Batch &b, double value, cudaStream_t s);
+int launch_advance_time(const Batch &b, cudaStream_t s);
 
 // Kinetic (CFL-less) path.  The kinetic state is stored in sweep order: item
 // k (its position in the level-sorted list of (element, velocity) pairs)
@@ -66,8 +78,8 @@ template <typename F, typename Y, typename T>
 int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cudaStream_t s);
 
 // f_eq of the analytic data at the boundary face nodes, t + dt/2 (FP64)
-int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double dt,
-							  int nv, const double *vi, double feq_c, double *bt, cudaStream_t s);
+int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Batch &b, int nv, const double *vi,
+							  double feq_c, double *bt, cudaStream_t s);
 
 // FP64 residual r = f - b - M1 yacc of every item (b: inflow boundary data)
 struct KinResidualParams {

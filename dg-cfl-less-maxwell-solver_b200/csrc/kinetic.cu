@@ -79,7 +79,8 @@ __global__ void kin_mask_kernel(const double *__restrict__ sown64, const int *__
 // pivoting, written at the item's sweep position with theta dt / det.
 template <typename GT>
 __global__ void kin_blocks_kernel(const double *__restrict__ geom, const double *__restrict__ sown64,
-								  const int *__restrict__ pos, long long ne, KinModel km, double theta_dt,
+								  const int *__restrict__ pos, long long ne, KinModel km, double theta,
+								  const int *__restrict__ einst, const double *__restrict__ dt_tab,
 								  GT *__restrict__ G, GT *__restrict__ rcoef, double4 *__restrict__ ru64,
 								  double4 *__restrict__ rs64, int *__restrict__ bad)
 {
@@ -112,7 +113,7 @@ __global__ void kin_blocks_kernel(const double *__restrict__ geom, const double 
 			for (int jj = 0; jj < 6; jj++)
 				F[tb.f2n[f][ii]][tb.f2n[f][jj]] += sp * tb.S[ii][jj];
 	}
-	const double c = theta_dt / det;
+	const double c = theta * dt_tab[einst ? einst[e] : 0] / det;
 	double a[10][20];
 	for (int i = 0; i < 10; i++) {
 		for (int j = 0; j < 10; j++) {
@@ -205,12 +206,13 @@ int launch_kin_setup(const int *face2elem, long long nf, const double *geom, con
 
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
-					  const int *perm, long long ne, const KinModel &km, double theta_dt, GT *G, GT *rcoef,
-					  int4 *rnb, int4 *rpm, GT *rs, double4 *ru64, double4 *rs64, int *bad, cudaStream_t s)
+					  const int *perm, long long ne, const KinModel &km, double theta, const int *einst,
+					  const double *dt_tab, GT *G, GT *rcoef, int4 *rnb, int4 *rpm, GT *rs, double4 *ru64,
+					  double4 *rs64, int *bad, cudaStream_t s)
 {
 	const long long nu = ne * km.nv;
-	kin_blocks_kernel<GT><<<(unsigned)((nu + 127) / 128), 128, 0, s>>>(geom, sown64, pos, ne, km, theta_dt, G, rcoef,
-																	   ru64, rs64, bad);
+	kin_blocks_kernel<GT><<<(unsigned)((nu + 127) / 128), 128, 0, s>>>(geom, sown64, pos, ne, km, theta, einst,
+																	   dt_tab, G, rcoef, ru64, rs64, bad);
 	GDN_CUDA_TRY(cudaGetLastError());
 	kin_records_kernel<GT><<<(unsigned)((nu + 255) / 256), 256, 0, s>>>(items, pos, sown64, nb, perm, nu, km.nv, rnb,
 																		rpm, rs);
@@ -220,17 +222,18 @@ int launch_kin_blocks(const double *geom, const double *sown64, const int *items
 template int launch_kin_setup<double>(const int *, long long, const double *, const int *, long long,
 									  const KinModel &, double *, unsigned char *, cudaStream_t);
 template int launch_kin_blocks<double>(const double *, const double *, const int *, const int *, const int *,
-									   const int *, long long, const KinModel &, double, double *, double *, int4 *,
-									   int4 *, double *, double4 *, double4 *, int *, cudaStream_t);
+									   const int *, long long, const KinModel &, double, const int *, const double *,
+									   double *, double *, int4 *, int4 *, double *, double4 *, double4 *, int *,
+									   cudaStream_t);
 template int launch_kin_blocks<float>(const double *, const double *, const int *, const int *, const int *,
-									  const int *, long long, const KinModel &, double, float *, float *, int4 *,
-									  int4 *, float *, double4 *, double4 *, int *, cudaStream_t);
+									  const int *, long long, const KinModel &, double, const int *, const double *,
+									  float *, float *, int4 *, int4 *, float *, double4 *, double4 *, int *,
+									  cudaStream_t);
 
 // f_eq of the analytic data at every boundary face node for every velocity,
 // at t + dt/2 (relaxation.c:99, dg_update_boundary with use_feq), formed from
 // the device time with the host's rounding.  bt[((bf * nv + v) * 6 + c) * 6 + jj].
-__global__ void kin_boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Data d,
-										  const double *__restrict__ t_dev, double dt, KinModel km,
+__global__ void kin_boundary_trace_kernel(const double *__restrict__ bxyz, long long nbf, Batch b, KinModel km,
 										  double *__restrict__ bt)
 {
 	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -238,9 +241,10 @@ __global__ void kin_boundary_trace_kernel(const double *__restrict__ bxyz, long 
 		return;
 	const long long bf = u / 6;
 	const int jj = (int)(u % 6);
-	const double t_half = __dadd_rn(*t_dev, __dmul_rn(0.5, dt));
+	const int inst = b.bfinst ? b.bfinst[bf] : 0;
+	const double t_half = __dadd_rn(b.t[inst], __dmul_rn(0.5, b.dt[inst]));
 	double x[3] = {bxyz[3 * u], bxyz[3 * u + 1], bxyz[3 * u + 2]}, we[6], Aw[6];
-	exact_w(d, x, t_half, we);
+	exact_w(b.data[inst], x, t_half, we);
 	for (int v = 0; v < km.nv; v++) {
 		double n[3] = {km.vi[3 * v], km.vi[3 * v + 1], km.vi[3 * v + 2]};
 		maxwell_A<double>(n, we, Aw);
@@ -249,8 +253,8 @@ __global__ void kin_boundary_trace_kernel(const double *__restrict__ bxyz, long 
 	}
 }
 
-int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Data &d, const double *t_dev, double dt,
-							  int nv, const double *vi, double feq_c, double *bt, cudaStream_t s)
+int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Batch &b, int nv, const double *vi,
+							  double feq_c, double *bt, cudaStream_t s)
 {
 	if (nbf <= 0)
 		return GDN_CUDA_OK;
@@ -259,7 +263,7 @@ int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Data &d, 
 	for (int i = 0; i < 3 * NV_MAX; i++)
 		km.vi[i] = vi[i];
 	km.feq_c = feq_c;
-	kin_boundary_trace_kernel<<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, d, t_dev, dt, km, bt);
+	kin_boundary_trace_kernel<<<(unsigned)((nbf * 6 + 255) / 256), 256, 0, s>>>(bxyz, nbf, b, km, bt);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }

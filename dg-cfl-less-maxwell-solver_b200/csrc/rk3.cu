@@ -346,7 +346,8 @@ __global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
 			}
 		}
 		const T inv_det = T(1) / sG[9 * P + e];
-		const T A = (T)p.A, B = (T)p.B, dt = (T)p.dt;
+		const T A = (T)p.A, B = (T)p.B;
+		const T dt = p.einst ? (T)p.dt_tab[p.einst[e0 + e]] : (T)p.dt;
 		T dwv[10];
 		lift_minv<T>(tb, R, dwv);
 #pragma unroll

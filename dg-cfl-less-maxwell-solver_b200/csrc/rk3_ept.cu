@@ -165,7 +165,8 @@ __global__ void __launch_bounds__(kEptTile) rk3_stage_ept_kernel(Rk3Params<T> p)
 	__syncthreads();
 	if (live) {
 		const T inv_det = T(1) / det;
-		const T A = (T)p.A, B = (T)p.B, dt = (T)p.dt;
+		const T A = (T)p.A, B = (T)p.B;
+		const T dt = p.einst ? (T)p.dt_tab[p.einst[e0 + e]] : (T)p.dt;
 #pragma unroll
 		for (int c = 0; c < 6; c++) {
 #pragma unroll

@@ -122,6 +122,34 @@ def random_plane_wave(seed: int, kmag: float):
     return k, float(kmag), p
 
 
+def uneven_plane_wave_batch(seed: int, count: int, n_lo: int = 8, n_hi: int = 40, jitter: float = 0.1,
+                            kmag_lo: float = 2 * np.pi, kmag_hi: float = 8 * np.pi):
+    """Specs of `count` independent plane-wave solves of uneven size.
+
+    Instance i draws everything from z_i = splitmix64(seed + i): the cube
+    resolution n uniform in [n_lo, n_hi], the jitter seed z_i (jitter +/-J h),
+    and, from a Philox generator keyed by z_i, a unit wave direction (a
+    normalised Gaussian triple), |k| uniform in [kmag_lo, kmag_hi] and a
+    polarisation orthogonal to the direction.  Even i run RK3, odd i the
+    CFL-less scheme.  Returns a list of dicts.
+    """
+    out = []
+    z = splitmix64(np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + np.arange(count, dtype=np.uint64))
+    for i in range(count):
+        zi = int(z[i])
+        n = n_lo + zi % (n_hi - n_lo + 1)
+        rng = np.random.Generator(np.random.Philox(zi))
+        k = rng.standard_normal(3)
+        k /= np.linalg.norm(k)
+        kmag = kmag_lo + (kmag_hi - kmag_lo) * rng.random()
+        q = rng.standard_normal(3)
+        p = q - np.dot(q, k) * k
+        p /= np.linalg.norm(p)
+        out.append({"index": i, "n": int(n), "jitter": jitter, "jitter_seed": zi, "khat": k, "kmag": float(kmag),
+                    "pol": p, "scheme": "rk3" if i % 2 == 0 else "kinetic"})
+    return out
+
+
 def write_msh22(path: str, coords: np.ndarray, elem2node: np.ndarray) -> None:
     """gmsh v2.2 ASCII, 1-based, type-4 elements with two tags."""
     nv = len(coords)

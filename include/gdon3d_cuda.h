@@ -104,12 +104,17 @@ typedef struct gdn_cuda_model {
 
 #define GDN_CUDA_FP64 0 /* FP64 storage and arithmetic */
 #define GDN_CUDA_FP32 1 /* FP32 storage and arithmetic, FP64 setup and norms */
-#define GDN_CUDA_FP32_REFINE 2 /* kinetic: FP64 state, FP32 sweeps, FP64 residual refinement */
+#define GDN_CUDA_FP32_REFINE 2 /* kinetic: FP64 state and relaxation, FP32 sweeps,
+                                  FP64-residual correction sweeps */
 #define GDN_CUDA_BF16_STORE 3 /* kinetic: BF16 distributions, FP32 arithmetic */
 typedef struct gdn_cuda_config {
 	int precision;
-	int refine_passes; /* GDN_CUDA_FP32_REFINE: FP64-residual passes (1 or 2) */
-	int elems_per_cta; /* RK3 element tile; 0 = autotuned */
+	int refine_passes; /* GDN_CUDA_FP32_REFINE: FP64-residual correction passes
+	                      per transport solve, 0 to 4 */
+	int elems_per_cta; /* RK3 stage kernel: 32 (a warp per field of 32-element
+	                      tiles), 128 (a thread per element), 0 = the faster
+	                      of the two, timed at attach and cached per
+	                      (precision, mesh-size bucket) */
 	int use_graph; /* capture step loops as CUDA graphs (1 = yes) */
 	int device; /* CUDA device ordinal */
 } gdn_cuda_config;
@@ -150,6 +155,26 @@ int gdn_cuda_attach(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
 					const gdn_cuda_config *config, double dt,
 					gdn_cuda_handle **out);
 
+/* No counterpart in the reference (one gdn_simulation per run): a batch of
+ * independent solves in one handle.  Their meshes are concatenated on the
+ * device (a flattened element-offset table), every kernel launch of a stage
+ * or step covers all instances, and each instance keeps its own dt, analytic
+ * data and time.  All instances share the scheme and, for the kinetic scheme,
+ * the velocity model (nb_v, vi, lambda, omega, theta).  The batch state used by
+ * gdn_cuda_solve / set_state / get_state is the concatenation of the
+ * instances' reference-layout vectors (gdn_cuda_instance_info gives each
+ * instance's offset and length); gdn_cuda_get_time, gdn_cuda_error_l2 and the
+ * time returned by gdn_cuda_solve refer to instance 0. */
+typedef struct gdn_cuda_instance {
+	const gdn_cuda_mesh *mesh;
+	const gdn_cuda_model *model;
+	const gdn_cuda_data *data;
+	double dt;
+} gdn_cuda_instance;
+int gdn_cuda_attach_batch(const gdn_cuda_instance *inst, int ninst,
+						  const gdn_cuda_tables *tables,
+						  const gdn_cuda_config *config, gdn_cuda_handle **out);
+
 int gdn_cuda_detach(gdn_cuda_handle *h);
 
 /* ---- the path ---------------------------------------------------------- */
@@ -173,13 +198,16 @@ int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t);
 int gdn_cuda_get_state(gdn_cuda_handle *h, double *wn);
 
 /* One call a caller makes per chunk of a run: copies wn (host, reference
- * layout) to the device, advances nsteps, copies the result back into wn. */
+ * layout) to the device, advances nsteps, copies the result back into wn.
+ * Single-instance handles only. */
 int gdn_cuda_step_host(gdn_cuda_handle *h, double *wn, int nsteps);
 
 /* simulation_error_l2 (src/simulation/simulation.c:606-666) of the device
  * state at the current time: mean over the 6 fields of the nodal-quadrature
  * L2 norm of (w - w_exact).  FP64, deterministic. */
 int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err);
+/* the same norm for every instance of a batch: err[ninst] */
+int gdn_cuda_error_l2_batch(gdn_cuda_handle *h, double *err);
 
 /* No counterpart in the reference.  The same norm as gdn_cuda_error_l2 for
  * callers that cannot allocate device memory (code running under stream
@@ -200,6 +228,14 @@ int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, const double *
 
 /* ---- introspection ------------------------------------------------------ */
 int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
+int gdn_cuda_num_instances(gdn_cuda_handle *h, int *ninst);
+/* RK3: the stage kernel's element tile in use (32 or 128; 0 for kinetic) */
+int gdn_cuda_rk3_tile(gdn_cuda_handle *h, int *elems_per_cta);
+/* instance i of a batch: its time, element count and the offset / length of
+ * its reference-layout state in the batch state vector (any output may be
+ * NULL) */
+int gdn_cuda_instance_info(gdn_cuda_handle *h, int i, double *t, long long *nbelems,
+						   long long *w_offset, long long *wlen);
 /* wlen = m * neq of the reference layout */
 int gdn_cuda_state_size(gdn_cuda_handle *h, long long *wlen);
 /* kinetic: number of sweep levels of the schedule (0 for RK3) */

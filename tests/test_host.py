@@ -136,3 +136,29 @@ def test_random_plane_wave_is_orthonormal():
     k, kmag, p = kuhn.random_plane_wave(3, 4 * np.pi)
     assert abs(np.linalg.norm(k) - 1) < 1e-15 and abs(np.linalg.norm(p) - 1) < 1e-15
     assert abs(np.dot(k, p)) < 1e-15 and kmag == 4 * np.pi
+
+
+def test_batch_attach_validates_instances():
+    """A batch needs one scheme (and one kinetic model) for all instances;
+    the check happens before any device call."""
+    c, e = kuhn.kuhn_cube(2)
+    m = capi.mesh_build(c, e)
+    L = capi.lib()
+    tabs = capi.t10_tables()
+    vi = np.zeros(3)
+    rk3 = capi.Model(capi.SCHEME_RK3, 6, 0, 1.0, 0.0, capi._dp(vi), 0.5)
+    vk = np.ascontiguousarray((capi.D3Q4_VI * capi.D3Q4_LAMBDA).ravel())
+    kin = capi.Model(capi.SCHEME_KINETIC, 6, 4, capi.D3Q4_LAMBDA, capi.RELAX_OMEGA, capi._dp(vk), 0.5)
+    d = capi.plane_data()
+    inst = (capi.Instance * 2)()
+    for i, mod in enumerate((rk3, kin)):
+        inst[i].mesh = C.pointer(m.struct)
+        inst[i].model = C.pointer(mod)
+        inst[i].data = C.pointer(d)
+        inst[i].dt = 0.01
+    h = C.c_void_p()
+    rc = L.gdn_cuda_attach_batch(inst, 2, C.byref(tabs), None, C.byref(h))
+    assert rc == capi.ERR_UNSUPPORTED
+    assert "one scheme" in L.gdn_cuda_last_error().decode()
+    rc = L.gdn_cuda_attach_batch(inst, 0, C.byref(tabs), None, C.byref(h))
+    assert rc == capi.ERR_INVALID
