@@ -109,6 +109,13 @@ struct gdn_cuda_handle {
 	double *yacc = nullptr; // FP32_REFINE: FP64 solution of the transport solve
 	float *rhs = nullptr; // FP32_REFINE: residual, right-hand side of the corrections
 	int refine_passes = 1;
+	int kin_mode = 1; // 1: a launch per sweep level, 2: one cooperative launch per sweep
+	bool kin_autotune = true; // pick kin_mode at attach by timing both
+	int kin_grid[3] = {0, 0, 0}; // CTAs of the cooperative sweep, per accumulate mode
+	int max_chunks = 1; // most 32-item chunks in one level
+	int *level_off_dev = nullptr;
+	unsigned *bar = nullptr; // [2] grid barrier of the cooperative sweep
+	int *err = nullptr; // set on the device when a barrier wait gave up
 	int *items = nullptr; // [k] e * nv + v
 	int *pos = nullptr; // [e * nv + v] k
 	std::vector<int> level_off;
@@ -504,6 +511,9 @@ static int autotune_rk3(gdn_cuda_handle *h)
 	return GDN_CUDA_OK;
 }
 
+static int kin_prepare_grids(gdn_cuda_handle *h);
+static int autotune_kin(gdn_cuda_handle *h);
+
 static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cuda_tables *t,
 					   const gdn_cuda_model *mo)
 {
@@ -674,6 +684,23 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		if (bad)
 			return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: a transport diagonal block is singular");
 		GDN_TRY(dalloc(h, &h->staging, (long long)6 * nv * h->neq));
+		// the cooperative sweep: level table, barrier, error flag, grids
+		const int nl = (int)h->level_off.size() - 1;
+		GDN_TRY(dalloc(h, &h->level_off_dev, nl + 1));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->level_off_dev, h->level_off.data(), (nl + 1) * sizeof(int),
+									 cudaMemcpyHostToDevice, s));
+		GDN_TRY(dalloc(h, &h->bar, 2));
+		GDN_TRY(dalloc(h, &h->err, 1));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned), s));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
+		for (int l = 0; l < nl; l++) {
+			const int nch = (h->level_off[l + 1] - h->level_off[l] + 31) / 32;
+			h->max_chunks = nch > h->max_chunks ? nch : h->max_chunks;
+		}
+		GDN_TRY(kin_prepare_grids(h));
+		GDN_CUDA_TRY(cudaStreamSynchronize(s));
+		if (h->kin_autotune)
+			GDN_TRY(autotune_kin(h));
 	}
 	return GDN_CUDA_OK;
 }
@@ -802,13 +829,15 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: no instances");
 	if (!tables)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: tables missing");
-	gdn_cuda_config cfg = {GDN_CUDA_FP64, 1, 0, 1, 0};
+	gdn_cuda_config cfg = {GDN_CUDA_FP64, 1, 0, 1, 0, 0};
 	if (config)
 		cfg = *config;
 	if (cfg.precision < GDN_CUDA_FP64 || cfg.precision > GDN_CUDA_BF16_STORE)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
 	if (cfg.elems_per_cta != 0 && cfg.elems_per_cta != 32 && cfg.elems_per_cta != 128)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: elems_per_cta must be 0 (auto), 32 or 128");
+	if (cfg.kin_sweep < 0 || cfg.kin_sweep > 2)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kin_sweep must be 0 (auto), 1 or 2");
 	for (int i = 0; i < n; i++) {
 		GDN_TRY(validate_mesh(inst[i].mesh));
 		GDN_TRY(validate_data(inst[i].data));
@@ -838,6 +867,8 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 	// tiles with a thread per element; 0 = timed at attach
 	h->rk3_variant = cfg.elems_per_cta == 128 ? 1 : 0;
 	h->rk3_autotune = cfg.elems_per_cta == 0;
+	h->kin_mode = cfg.kin_sweep == 2 ? 2 : 1;
+	h->kin_autotune = cfg.kin_sweep == 0;
 	h->ninst = n;
 	for (int i = 0; i < n; i++) {
 		h->hdata.push_back(to_data(inst[i].data));
@@ -975,6 +1006,16 @@ static int kin_sweeps(gdn_cuda_handle *h, const void *f, int acc, int bdata, lon
 	p.bt = h->bt;
 	p.nv = h->nv;
 	const int nl = (int)h->level_off.size() - 1;
+	if (h->kin_mode == 2) {
+		int grid = h->kin_grid[acc] < h->max_chunks ? h->kin_grid[acc] : h->max_chunks;
+		grid = grid > 0 ? grid : 1;
+		p.item_begin = 0;
+		p.item_end = h->level_off[nl];
+		GDN_TRY((launch_kin_levels<F, Y, T>(p, h->level_off_dev, nl, grid, h->bar, h->err, acc, bdata, h->rk3_sparse,
+											h->stream)));
+		nlaunch++;
+		return GDN_CUDA_OK;
+	}
 	for (int l = 0; l < nl; l++) {
 		p.item_begin = h->level_off[l];
 		p.item_end = h->level_off[l + 1];
@@ -1051,6 +1092,123 @@ static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 	}
 	GDN_TRY(launch_advance_time(h->batch(), h->stream));
 	nlaunch++;
+	return GDN_CUDA_OK;
+}
+
+// CTAs of the cooperative sweep for the variants this handle's precision runs
+static int kin_prepare_grids(gdn_cuda_handle *h)
+{
+	const int sp = h->rk3_sparse;
+	switch (h->precision) {
+	case GDN_CUDA_FP64:
+		return kin_levels_grid<double, double, double>(h->device, 0, sp, &h->kin_grid[0]);
+	case GDN_CUDA_FP32:
+		return kin_levels_grid<float, float, float>(h->device, 0, sp, &h->kin_grid[0]);
+	case GDN_CUDA_BF16_STORE:
+		return kin_levels_grid<__nv_bfloat16, float, float>(h->device, 0, sp, &h->kin_grid[0]);
+	default:
+		GDN_TRY((kin_levels_grid<double, float, float>(h->device, 1, sp, &h->kin_grid[1])));
+		return kin_levels_grid<float, float, float>(h->device, 2, sp, &h->kin_grid[2]);
+	}
+}
+
+// the first transport solve of a step, as the step runs it
+static int kin_first_sweep(gdn_cuda_handle *h, long long &nl)
+{
+	switch (h->precision) {
+	case GDN_CUDA_FP64:
+		return kin_sweeps<double, double, double>(h, h->f, 0, 1, nl);
+	case GDN_CUDA_FP32:
+		return kin_sweeps<float, float, float>(h, h->f, 0, 1, nl);
+	case GDN_CUDA_BF16_STORE:
+		return kin_sweeps<__nv_bfloat16, float, float>(h, h->f, 0, 1, nl);
+	default:
+		return kin_sweeps<double, float, float>(h, h->f, 1, 1, nl);
+	}
+}
+
+// Sweep-level grouping autotuner: times one transport solve with a launch per
+// level and as one cooperative launch over all levels on the handle's own
+// buffers (their contents do not change the work; init / set_state rewrite
+// them) and keeps the faster.  Cached per (precision, floor(log2 items),
+// floor(log2 levels)) for the life of the process.
+static std::map<std::pair<int, int>, int> g_tune_kin;
+
+static int autotune_kin(gdn_cuda_handle *h)
+{
+	int ib = 0, lb = 0;
+	const long long nitems = h->ne * h->nv;
+	const long long nl = (long long)h->level_off.size() - 1;
+	while ((2LL << ib) <= nitems)
+		ib++;
+	while ((2LL << lb) <= nl)
+		lb++;
+	const std::pair<int, int> key(h->precision, ib * 64 + lb);
+	{
+		std::lock_guard<std::mutex> g(g_tune_mu);
+		auto it = g_tune_kin.find(key);
+		if (it != g_tune_kin.end()) {
+			h->kin_mode = it->second;
+			return GDN_CUDA_OK;
+		}
+	}
+	GDN_CUDA_TRY(cudaMemsetAsync(h->f, 0, (size_t)60 * nitems * (h->precision == GDN_CUDA_FP32 ? 4 : h->precision == GDN_CUDA_BF16_STORE ? 2 : 8), h->stream));
+	GDN_CUDA_TRY(cudaMemsetAsync(h->bt, 0, (size_t)36 * h->nv * (h->nbf > 0 ? h->nbf : 1) * sizeof(double), h->stream));
+	cudaEvent_t ev[2];
+	GDN_CUDA_TRY(cudaEventCreate(&ev[0]));
+	GDN_CUDA_TRY(cudaEventCreate(&ev[1]));
+	float best = 0.f;
+	int pick = 1, rc = GDN_CUDA_OK;
+	for (int mode = 1; mode <= 2 && rc == GDN_CUDA_OK; mode++) {
+		h->kin_mode = mode;
+		long long nlaunch = 0;
+		rc = kin_first_sweep(h, nlaunch); // warm-up
+		if (rc != GDN_CUDA_OK)
+			break;
+		cudaEventRecord(ev[0], h->stream);
+		for (int rep = 0; rep < 2 && rc == GDN_CUDA_OK; rep++)
+			rc = kin_first_sweep(h, nlaunch);
+		h->launches += nlaunch;
+		if (rc != GDN_CUDA_OK)
+			break;
+		cudaEventRecord(ev[1], h->stream);
+		float ms = 0.f;
+		cudaError_t e = cudaEventSynchronize(ev[1]);
+		if (e == cudaSuccess)
+			e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+		if (e != cudaSuccess)
+			rc = gdn_cuda_fail(e, "autotune_kin", __FILE__, __LINE__);
+		if (mode == 1 || ms < best) {
+			best = ms;
+			pick = mode;
+		}
+	}
+	cudaEventDestroy(ev[0]);
+	cudaEventDestroy(ev[1]);
+	if (rc != GDN_CUDA_OK)
+		return rc;
+	h->kin_mode = pick;
+	std::lock_guard<std::mutex> g(g_tune_mu);
+	g_tune_kin[key] = pick;
+	return GDN_CUDA_OK;
+}
+
+// A cooperative sweep whose bounded barrier wait gave up leaves *err set: the
+// state is invalid; report it (and clear the flag) at the next synchronising
+// call.
+static int check_device_error(gdn_cuda_handle *h)
+{
+	if (!h->err)
+		return GDN_CUDA_OK;
+	int e = 0;
+	GDN_CUDA_TRY(cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	if (e) {
+		GDN_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned), h->stream));
+		GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+		return gdn_set_error(GDN_CUDA_ERR_TIMEOUT, "kinetic sweep: a grid barrier wait timed out; the state is invalid");
+	}
 	return GDN_CUDA_OK;
 }
 
@@ -1241,6 +1399,7 @@ extern "C" int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t
 
 static int get_state_impl(gdn_cuda_handle *h, double *wn)
 {
+	GDN_TRY(check_device_error(h));
 	cudaStream_t s = h->stream;
 	for (int i = 0; i < h->ninst; i++) {
 		const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
@@ -1318,6 +1477,7 @@ extern "C" int gdn_cuda_solve(gdn_cuda_handle *h, int itermax, double *wn, doubl
 // simulation_error_l2 of instance i at its current time
 static int error_l2_impl(gdn_cuda_handle *h, int i, double *err)
 {
+	GDN_TRY(check_device_error(h));
 	cudaStream_t s = h->stream;
 	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
 	const int sk = kin ? kin_state_kind(h) : (h->precision == GDN_CUDA_FP64 ? 0 : 1);
@@ -1368,6 +1528,14 @@ extern "C" int gdn_cuda_get_time(gdn_cuda_handle *h, double *t)
 	if (!h || !t)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "get_time: bad arguments");
 	*t = h->ht[0];
+	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode)
+{
+	if (!h || !mode)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "kin_sweep_mode: bad arguments");
+	*mode = h->scheme == GDN_CUDA_SCHEME_KINETIC ? h->kin_mode : 0;
 	return GDN_CUDA_OK;
 }
 

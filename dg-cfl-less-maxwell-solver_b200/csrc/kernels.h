@@ -77,6 +77,15 @@ struct KinSweepParams {
 template <typename F, typename Y, typename T>
 int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cudaStream_t s);
 
+// The same solve as one cooperative launch walking all levels with a grid
+// barrier between them (grid = CTAs resident at once, kin_levels_grid); a
+// barrier that times out sets *err.
+template <typename F, typename Y, typename T>
+int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels, int grid, unsigned *bar, int *err,
+					  int acc, int bdata, int sparse, cudaStream_t s);
+template <typename F, typename Y, typename T>
+int kin_levels_grid(int device, int acc, int sparse, int *grid);
+
 // f_eq of the analytic data at the boundary face nodes, t + dt/2 (FP64)
 int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Batch &b, int nv, const double *vi,
 							  double feq_c, double *bt, cudaStream_t s);

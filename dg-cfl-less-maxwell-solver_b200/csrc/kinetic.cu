@@ -343,18 +343,18 @@ struct SweepG {
 	static constexpr int per_vec = 16 / sizeof(T);
 };
 
-template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE>
-__global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
+// 32 consecutive items [k0, min(k0 + 32, item_end)) of one level.  `wait` is
+// called after the prologue (records, right-hand side, G staging: data no
+// sweep level writes) and before the first trace load.  L2 = true reads the
+// traces through L2 only (L1 is not coherent with other SMs' writes made
+// during the same launch).
+template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE, bool L2, typename Wait>
+__device__ __forceinline__ void sweep_chunk(const KinSweepParams &p, long long k0, long long item_end, T *gsh,
+											Wait wait)
 {
 	typedef SweepG<T> SG;
-	__shared__ __align__(16) T gsh[kSwItems * SG::stride];
-	// Programmatic dependent launch: the next level's CTAs may start now and
-	// run their prologue (everything below up to griddepcontrol.wait reads
-	// only data that no sweep level writes).
-	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
-	const long long k0 = (long long)p.item_begin + (long long)blockIdx.x * kSwItems;
-	const long long rem = (long long)p.item_end - k0;
+	const long long rem = item_end - k0;
 	const int nloc = rem < kSwItems ? (int)rem : kSwItems;
 	{
 		constexpr int VPC = SG::per_vec, CH = 100 / VPC;
@@ -389,9 +389,7 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 	int v = 0;
 	if (BD)
 		v = p.items[k] % p.nv;
-	// the upwind items of earlier levels are complete once the previous
-	// level's grid is
-	asm volatile("griddepcontrol.wait;" ::: "memory");
+	wait();
 	T r[10];
 	{
 		T tr[4][6];
@@ -401,8 +399,10 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 			if (nbv >= 0) {
 				const Y *yn = reinterpret_cast<const Y *>(p.y) + (long long)nbv * 60 + c * 10;
 #pragma unroll
-				for (int jj = 0; jj < 6; jj++)
-					tr[f][jj] = (T)Store<Y>::load(yn + ((pmk[f] >> (4 * jj)) & 15));
+				for (int jj = 0; jj < 6; jj++) {
+					const Y *q = yn + ((pmk[f] >> (4 * jj)) & 15);
+					tr[f][jj] = (T)(L2 ? Store<Y>::load_l2(q) : Store<Y>::load(q));
+				}
 			} else if (BD && nbv != INT_MIN) {
 				const double *b = p.bt + (((long long)(-nbv - 1) * p.nv + v) * 6 + c) * 6;
 #pragma unroll
@@ -442,31 +442,112 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 	}
 	__pipeline_wait_prior(0);
 	__syncthreads();
-	if (!act)
-		return;
-	T y[10];
-#pragma unroll
-	for (int i = 0; i < 10; i++)
-		y[i] = T(0);
-	const typename SG::vec *g = reinterpret_cast<const typename SG::vec *>(gsh + lane * SG::stride);
-#pragma unroll
-	for (int q = 0; q < 100 / SG::per_vec; q++) {
-		const typename SG::vec gv = g[q];
-		const T *ge = reinterpret_cast<const T *>(&gv);
-#pragma unroll
-		for (int u = 0; u < SG::per_vec; u++) {
-			const int idx = q * SG::per_vec + u;
-			y[idx / 10] += ge[u] * r[idx % 10];
-		}
-	}
-	store10<Y, T>(reinterpret_cast<Y *>(p.y) + k * 60 + c * 10, y);
-	if (ACC == 1) {
-		store10<double, T>(p.yacc + k * 60 + c * 10, y);
-	} else if (ACC == 2) {
+	if (act) {
+		T y[10];
 #pragma unroll
 		for (int i = 0; i < 10; i++)
-			ya[i] += (double)y[i];
-		store10<double, double>(p.yacc + k * 60 + c * 10, ya);
+			y[i] = T(0);
+		const typename SG::vec *g = reinterpret_cast<const typename SG::vec *>(gsh + lane * SG::stride);
+#pragma unroll
+		for (int q = 0; q < 100 / SG::per_vec; q++) {
+			const typename SG::vec gv = g[q];
+			const T *ge = reinterpret_cast<const T *>(&gv);
+#pragma unroll
+			for (int u = 0; u < SG::per_vec; u++) {
+				const int idx = q * SG::per_vec + u;
+				y[idx / 10] += ge[u] * r[idx % 10];
+			}
+		}
+		store10<Y, T>(reinterpret_cast<Y *>(p.y) + k * 60 + c * 10, y);
+		if (ACC == 1) {
+			store10<double, T>(p.yacc + k * 60 + c * 10, y);
+		} else if (ACC == 2) {
+#pragma unroll
+			for (int i = 0; i < 10; i++)
+				ya[i] += (double)y[i];
+			store10<double, double>(p.yacc + k * 60 + c * 10, ya);
+		}
+	}
+	// gsh is reused by the CTA's next chunk
+	__syncthreads();
+}
+
+template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE>
+__global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
+{
+	__shared__ __align__(16) T gsh[kSwItems * SweepG<T>::stride];
+	// Programmatic dependent launch: the next level's CTAs may start now and
+	// run their prologue (everything before griddepcontrol.wait reads only
+	// data that no sweep level writes).
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+	const long long k0 = (long long)p.item_begin + (long long)blockIdx.x * kSwItems;
+	// the upwind items of earlier levels are complete once the previous
+	// level's grid is
+	sweep_chunk<F, Y, T, ACC, BD, SPARSE, false>(p, k0, p.item_end, gsh,
+												[] { asm volatile("griddepcontrol.wait;" ::: "memory"); });
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs co-resident).  *count
+// only grows during the launch (it is cleared before the launch): barrier j
+// is passed once it reaches (j + 1) x gridDim.x arrivals.  Arrivals are
+// release-ordered, polls acquire-ordered.  The wait is bounded: after
+// spin_limit polls the CTA sets *err and leaves, and so does every other CTA
+// once it sees *err, so a lost CTA ends the launch instead of hanging it.
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, int *err, long long spin_limit)
+{
+	__shared__ int s_ok;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		volatile int *verr = err;
+		int ok = 1;
+		asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+		long long it = 0;
+		for (;;) {
+			unsigned v;
+			asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+			if (v >= target)
+				break;
+			if (*verr || ++it > spin_limit) {
+				atomicExch(err, 1);
+				ok = 0;
+				break;
+			}
+			__nanosleep(16);
+		}
+		s_ok = ok && !*verr;
+	}
+	__syncthreads();
+	return s_ok != 0;
+}
+
+// All levels of one transport solve in one cooperative launch: the CTAs walk
+// the levels in order, 32 items per chunk, with a grid barrier between levels.
+// A CTA stages its first chunk of level l (G, records, right-hand side) before
+// it waits at the barrier that ends level l - 1.
+template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE>
+__global__ void __launch_bounds__(kSwThreads) kin_levels_kernel(KinSweepParams p, const int *__restrict__ level_off,
+																	int nlevels, unsigned *bar, int *err,
+																	long long spin_limit)
+{
+	__shared__ __align__(16) T gsh[kSwItems * SweepG<T>::stride];
+	for (int l = 0; l < nlevels; l++) {
+		const long long b = level_off[l], e = level_off[l + 1];
+		const long long nch = (e - b + kSwItems - 1) / kSwItems;
+		bool pending = l > 0; // the barrier ending level l - 1 is still to pass
+		bool ok = true;
+		const unsigned target = (unsigned)l * gridDim.x;
+		for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+			sweep_chunk<F, Y, T, ACC, BD, SPARSE, true>(p, b + ch * kSwItems, e, gsh, [&] {
+				if (pending) {
+					ok = grid_barrier(bar, target, err, spin_limit);
+					pending = false;
+				}
+			});
+			if (!ok)
+				return;
+		}
+		if (pending && !grid_barrier(bar, target, err, spin_limit))
+			return;
 	}
 }
 
@@ -509,6 +590,77 @@ int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cu
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
+template <typename F, typename Y, typename T>
+int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels, int grid, unsigned *bar, int *err,
+					  int acc, int bdata, int sparse, cudaStream_t s)
+{
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)grid);
+	cfg.blockDim = dim3(kSwThreads);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = s;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	const long long spin = 1LL << 21; // each poll is an L2 round trip: a lost CTA ends the launch in ~1 s
+	GDN_CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(unsigned), s));
+#define GDN_LEVELS(A, B, SP)                                                                                          \
+	GDN_CUDA_TRY(cudaLaunchKernelEx(&cfg, kin_levels_kernel<F, Y, T, A, B, SP>, p, level_off, nlevels, bar, err, spin))
+	if (acc == 0 && bdata) {
+		if (sparse)
+			GDN_LEVELS(0, true, true);
+		else
+			GDN_LEVELS(0, true, false);
+	} else if (acc == 1 && bdata) {
+		if (sparse)
+			GDN_LEVELS(1, true, true);
+		else
+			GDN_LEVELS(1, true, false);
+	} else if (acc == 2 && !bdata) {
+		if (sparse)
+			GDN_LEVELS(2, false, true);
+		else
+			GDN_LEVELS(2, false, false);
+	} else {
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "kinetic sweep: unsupported accumulate / boundary mode");
+	}
+#undef GDN_LEVELS
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+
+// CTAs of the persistent level loop that fit on the device at once
+template <typename F, typename Y, typename T>
+int kin_levels_grid(int device, int acc, int sparse, int *grid)
+{
+	int nsm = 0, per = 0;
+	GDN_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+	const void *fn;
+	if (sparse)
+		fn = acc == 0   ? (const void *)kin_levels_kernel<F, Y, T, 0, true, true>
+			 : acc == 1 ? (const void *)kin_levels_kernel<F, Y, T, 1, true, true>
+						: (const void *)kin_levels_kernel<F, Y, T, 2, false, true>;
+	else
+		fn = acc == 0   ? (const void *)kin_levels_kernel<F, Y, T, 0, true, false>
+			 : acc == 1 ? (const void *)kin_levels_kernel<F, Y, T, 1, true, false>
+						: (const void *)kin_levels_kernel<F, Y, T, 2, false, false>;
+	GDN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kSwThreads, 0));
+	*grid = nsm * per;
+	return GDN_CUDA_OK;
+}
+
+#define GDN_LEVELS_INST(F, Y, T)                                                                                      \
+	template int launch_kin_levels<F, Y, T>(const KinSweepParams &, const int *, int, int, unsigned *, int *, int, int,  \
+											int, cudaStream_t);                                                          \
+	template int kin_levels_grid<F, Y, T>(int, int, int, int *);
+GDN_LEVELS_INST(double, double, double)
+GDN_LEVELS_INST(float, float, float)
+GDN_LEVELS_INST(__nv_bfloat16, float, float)
+GDN_LEVELS_INST(double, float, float)
+#undef GDN_LEVELS_INST
+
 template int launch_kin_sweep<double, double, double>(const KinSweepParams &, int, int, int, cudaStream_t);
 template int launch_kin_sweep<float, float, float>(const KinSweepParams &, int, int, int, cudaStream_t);
 template int launch_kin_sweep<__nv_bfloat16, float, float>(const KinSweepParams &, int, int, int, cudaStream_t);

@@ -117,6 +117,10 @@ typedef struct gdn_cuda_config {
 	                      (precision, mesh-size bucket) */
 	int use_graph; /* capture step loops as CUDA graphs (1 = yes) */
 	int device; /* CUDA device ordinal */
+	int kin_sweep; /* kinetic transport solve: 1 = a launch per sweep level,
+	                  2 = one cooperative launch walking all levels with a
+	                  grid barrier between them, 0 = the faster of the two,
+	                  timed at attach and cached per (precision, size) */
 } gdn_cuda_config;
 
 typedef struct gdn_cuda_handle gdn_cuda_handle;
@@ -229,6 +233,8 @@ int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, const double *
 /* ---- introspection ------------------------------------------------------ */
 int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
 int gdn_cuda_num_instances(gdn_cuda_handle *h, int *ninst);
+/* kinetic: the sweep mode in use (1 or 2, see kin_sweep; 0 for RK3) */
+int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode);
 /* RK3: the stage kernel's element tile in use (32 or 128; 0 for kinetic) */
 int gdn_cuda_rk3_tile(gdn_cuda_handle *h, int *elems_per_cta);
 /* instance i of a batch: its time, element count and the offset / length of

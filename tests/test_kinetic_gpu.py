@@ -168,3 +168,24 @@ def test_kinetic_bf16_storage_error_is_bounded():
     rel = np.linalg.norm(out["bf16"][0] - ref) / np.linalg.norm(ref)
     assert 1e-4 < rel < 2e-2, rel
     assert abs(out["bf16"][1] - out["fp64"][1]) <= 0.1 * out["fp64"][1]
+
+
+@pytest.mark.parametrize("precision,nb_v", [(capi.FP64, 4), (capi.FP32, 6), (capi.FP32_REFINE, 4),
+                                            (capi.BF16_STORE, 4)])
+def test_kinetic_cooperative_sweep_equals_level_launches(precision, nb_v):
+    """One cooperative launch walking all sweep levels (grid barrier between
+    levels) does per item the arithmetic of one launch per level: identical
+    states."""
+    c, e = kuhn.kuhn_cube(5, 0.15, seed=8)
+    mesh = capi.mesh_build(c, e)
+    dt = 10 * 0.3 * mesh.hmin()
+    out = []
+    for mode in (1, 2):
+        s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, precision=precision, nb_v=nb_v,
+                        kin_sweep=mode)
+        assert s.kin_sweep_mode == mode
+        wn, t, _ = s.solve(6)
+        out.append((wn, t, s.error_l2()))
+        s.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
