@@ -291,8 +291,9 @@ def main():
     ap.add_argument("--count", type=int, default=BATCH_COUNT, help="batched: number of instances")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--tile", type=int, default=0, choices=[0, 32, 128],
-                    help="RK3 stage kernel: 32 = warp per field, 128 = thread per element, 0 = autotuned")
+    ap.add_argument("--variant", type=int, default=0, choices=[0, 1, 2],
+                    help="RK3 stage kernel: 1 / 2 = compiled for fewer / more resident CTAs per SM, "
+                         "0 = autotuned")
     ap.add_argument("--only", default="all",
                     help="profiling aid: comma-separated variants to run (rk3: fp64,fp32; kinetic: "
                          "fp64,fp32,fp32_refine1,fp32_refine2,bf16)")
@@ -346,7 +347,7 @@ def run_rk3(args, env):
         if not _wanted(args, name):
             continue
         s = capi.Solver(mesh, capi.SCHEME_RK3, data, dt, precision=prec, device=local,
-                        elems_per_cta=args.tile)
+                        rk3_variant=args.variant)
         st = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
         s.init()
         s.advance(W)
@@ -375,7 +376,7 @@ def run_rk3(args, env):
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg / 3,
                          "traffic": dram_traffic("rk3_stage_%s_n%d" % (name, n))},
-            "rk3_tile": s.rk3_tile, "solver": s}
+            "rk3_variant": s.rk3_variant, "solver": s}
     rel_fp32 = None
     if "fp64" in states and "fp32" in states:
         ref64 = states["fp64"][: 60 * ne]
@@ -427,7 +428,7 @@ def run_rk3(args, env):
                                % (60 * ne * 4 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single-gpu"},
         "roofline": head["roofline"], "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
-        "rk3_tile": head["rk3_tile"],
+        "rk3_variant": head["rk3_variant"],
         "l2_rel_fp32_vs_fp64": rel_fp32,
         "l2_error_vs_analytic": {k: v["l2_error_vs_analytic"] for k, v in results.items()},
         "variants": {k + ("_plain" if k == "fp64" else ""):
@@ -614,7 +615,7 @@ def run_batched(args, env, specs, built):
     ms_batch = env.max_over_ranks(max(ev0.elapsed_time(eva), ev0.elapsed_time(evb)))
     launches = brk.launches + bkn.launches - l0
     err_b = {"rk3": brk.error_l2_batch(), "kinetic": bkn.error_l2_batch()}
-    tile = brk.rk3_tile
+    tile = brk.rk3_variant
     levels = bkn.num_levels
     brk.close()
     bkn.close()
@@ -659,7 +660,7 @@ def run_batched(args, env, specs, built):
                    "elements_total": int(sum(ne)), "rk3_elements": int(sum(ne[i] for i in rk)),
                    "kinetic_elements": int(sum(ne[i] for i in kn)), "n_range": [8, 40], "jitter": 0.1,
                    "seed": SEED, "rk3_steps": BATCH_RK3_STEPS, "kinetic_steps": BATCH_KIN_STEPS,
-                   "kinetic_cfl_multiple": BATCH_KIN_MULT, "rk3_tile_autotuned": tile,
+                   "kinetic_cfl_multiple": BATCH_KIN_MULT, "rk3_variant_autotuned": tile,
                    "kinetic_levels": levels, "attach_s": attach_s,
                    "precision": "FP32 state and arithmetic; FP64 setup and norms",
                    "l2_flush": "inputs larger than L2 (%.1f GB of FP32 RK3 state)"

@@ -65,7 +65,7 @@ class Instance(C.Structure):
 
 
 class Config(C.Structure):
-    _fields_ = [("precision", C.c_int), ("refine_passes", C.c_int), ("elems_per_cta", C.c_int),
+    _fields_ = [("precision", C.c_int), ("refine_passes", C.c_int), ("rk3_variant", C.c_int),
                 ("use_graph", C.c_int), ("device", C.c_int), ("kin_sweep", C.c_int)]
 
 
@@ -75,7 +75,7 @@ EXPORTS = [
     "gdn_cuda_set_state", "gdn_cuda_get_state", "gdn_cuda_step_host", "gdn_cuda_error_l2",
     "gdn_cuda_get_time", "gdn_cuda_state_size", "gdn_cuda_num_levels", "gdn_cuda_launch_count",
     "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc", "gdn_cuda_attach_batch",
-    "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_tile",
+    "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_variant",
     "gdn_cuda_kin_sweep_mode",
 ]
 
@@ -115,7 +115,7 @@ def lib():
                                         C.POINTER(vp)]
     L.gdn_cuda_error_l2_batch.argtypes = [vp, dp]
     L.gdn_cuda_num_instances.argtypes = [vp, ip]
-    L.gdn_cuda_rk3_tile.argtypes = [vp, ip]
+    L.gdn_cuda_rk3_variant.argtypes = [vp, ip, ip]
     L.gdn_cuda_kin_sweep_mode.argtypes = [vp, ip]
     L.gdn_cuda_instance_info.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                          C.POINTER(C.c_longlong)]
@@ -242,7 +242,7 @@ class Solver:
 
     def __init__(self, mesh: MeshArrays, scheme=SCHEME_RK3, data: Data = None, dt: float = None,
                  precision=FP64, nb_v=4, tables: Tables = None, device=0, use_graph=1,
-                 refine_passes=1, theta=0.5, elems_per_cta=0, kin_sweep=0):
+                 refine_passes=1, theta=0.5, rk3_variant=0, kin_sweep=0):
         self.L = lib()
         self.h = C.c_void_p()
         self.mesh = mesh
@@ -250,7 +250,7 @@ class Solver:
         self.tables = tables if tables is not None else t10_tables()
         self.data = data if data is not None else plane_data()
         model = self._model(scheme, nb_v, theta)
-        cfg = Config(precision, refine_passes, elems_per_cta, use_graph, device, kin_sweep)
+        cfg = Config(precision, refine_passes, rk3_variant, use_graph, device, kin_sweep)
         check(self.L.gdn_cuda_attach(C.byref(mesh.struct), C.byref(self.tables), C.byref(model),
                                      C.byref(self.data), C.byref(cfg), float(dt), C.byref(self.h)))
         self.dt = float(dt)
@@ -326,10 +326,11 @@ class Solver:
         return n.value
 
     @property
-    def rk3_tile(self) -> int:
-        n = C.c_int()
-        check(self.L.gdn_cuda_rk3_tile(self.h, C.byref(n)))
-        return n.value
+    def rk3_variant(self):
+        """(variant in use, resident CTAs per SM it was compiled for)"""
+        v, m = C.c_int(), C.c_int()
+        check(self.L.gdn_cuda_rk3_variant(self.h, C.byref(v), C.byref(m)))
+        return v.value, m.value
 
     @property
     def launches(self) -> int:
@@ -361,7 +362,7 @@ class BatchSolver(Solver):
     each instance keeps its own mesh, data and dt."""
 
     def __init__(self, meshes, datas, dts, scheme=SCHEME_RK3, precision=FP64, nb_v=4, tables: Tables = None,
-                 device=0, use_graph=1, refine_passes=1, theta=0.5, elems_per_cta=0, kin_sweep=0):
+                 device=0, use_graph=1, refine_passes=1, theta=0.5, rk3_variant=0, kin_sweep=0):
         self.L = lib()
         self.h = C.c_void_p()
         self.meshes = list(meshes)
@@ -376,7 +377,7 @@ class BatchSolver(Solver):
             self._inst[i].model = C.pointer(model)
             self._inst[i].data = C.pointer(self.datas[i])
             self._inst[i].dt = float(dts[i])
-        cfg = Config(precision, refine_passes, elems_per_cta, use_graph, device, kin_sweep)
+        cfg = Config(precision, refine_passes, rk3_variant, use_graph, device, kin_sweep)
         check(self.L.gdn_cuda_attach_batch(self._inst, n, C.byref(self.tables), C.byref(cfg), C.byref(self.h)))
         self.dts = [float(d) for d in dts]
         self.dt = self.dts[0]

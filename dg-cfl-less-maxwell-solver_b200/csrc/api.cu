@@ -95,7 +95,7 @@ struct gdn_cuda_handle {
 	void *k2 = nullptr;
 	void *btrace = nullptr; // [nbf][6][6] boundary traces at the stage time
 	int cur = 0;
-	int rk3_variant = 0; // 0: field-per-warp tiles of 32, 1: element-per-thread tiles of 128
+	int rk3_variant = 0; // stage kernel for fewer (0) / more (1) resident CTAs per SM
 	bool rk3_autotune = true; // pick the variant at attach by timing both
 	// kinetic, in sweep order (item k = position in the level-sorted list)
 	// f: FP64 (FP64, FP32_REFINE), FP32 or BF16; y: FP64 or FP32; G, rs,
@@ -485,7 +485,7 @@ static int autotune_rk3(gdn_cuda_handle *h)
 		for (int rep = 0; rep < 4 && rc == GDN_CUDA_OK; rep++) { // launch 0 warms up
 			if (rep == 1)
 				cudaEventRecord(ev[0], h->stream);
-			rc = v == 0 ? launch_rk3_stage<T>(p, h->stream) : launch_rk3_stage_ept<T>(p, h->stream);
+			rc = launch_rk3_stage<T>(p, v, h->stream);
 			h->launches++;
 		}
 		if (rc != GDN_CUDA_OK)
@@ -585,40 +585,42 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		return gdn_set_error(GDN_CUDA_ERR_MESH, "attach: an element has a non-positive Jacobian determinant");
 
 	const bool fp64 = h->precision == GDN_CUDA_FP64;
-	if (fp64) {
-		h->geomT = h->geom64;
-	} else {
-		float *g32;
-		GDN_TRY(dalloc(h, &g32, 10 * ne));
-		GDN_TRY(launch_convert<float>(h->geom64, g32, 10 * ne, s));
-		h->launches++;
-		h->geomT = g32;
-	}
-
 	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
+		// state, k2 and geometry in tiles of 32 elements (the last one padded)
+		const long long nt = 32 * ((ne + 31) / 32);
 		h->neq = 10 * ne + 6 * nbf;
+		if (fp64) {
+			double *gt;
+			GDN_TRY(dalloc(h, &gt, 10 * nt));
+			GDN_TRY(launch_geom_to_tiles<double>(h->geom64, gt, ne, s));
+			h->geomT = gt;
+		} else {
+			float *gt;
+			GDN_TRY(dalloc(h, &gt, 10 * nt));
+			GDN_TRY(launch_geom_to_tiles<float>(h->geom64, gt, ne, s));
+			h->geomT = gt;
+		}
+		h->launches++;
 		GDN_TRY(prepare_rk3<double>());
 		GDN_TRY(prepare_rk3<float>());
-		GDN_TRY(prepare_rk3_ept<double>());
-		GDN_TRY(prepare_rk3_ept<float>());
 		if (fp64)
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->btrace), 36 * (nbf > 0 ? nbf : 1)));
 		else
 			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->btrace), 36 * (nbf > 0 ? nbf : 1)));
 		for (int b = 0; b < 2; b++) {
 			if (fp64)
-				GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->w[b]), 60 * ne));
+				GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->w[b]), 60 * nt));
 			else
-				GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->w[b]), 60 * ne));
+				GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->w[b]), 60 * nt));
 		}
 		if (fp64)
-			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->k2), 60 * ne));
+			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->k2), 60 * nt));
 		else
-			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->k2), 60 * ne));
-		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * ne * h->ssize, s));
+			GDN_TRY(dalloc(h, reinterpret_cast<float **>(&h->k2), 60 * nt));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * nt * h->ssize, s));
 		GDN_TRY(dalloc(h, &h->staging, 6 * h->neq));
 		if (h->rk3_autotune) {
-			GDN_CUDA_TRY(cudaMemsetAsync(h->w[0], 0, 60 * ne * h->ssize, s));
+			GDN_CUDA_TRY(cudaMemsetAsync(h->w[0], 0, 60 * nt * h->ssize, s));
 			GDN_CUDA_TRY(cudaMemsetAsync(h->btrace, 0, 36 * (nbf > 0 ? nbf : 1) * h->ssize, s));
 			if (fp64)
 				GDN_TRY(autotune_rk3<double>(h));
@@ -834,8 +836,8 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 		cfg = *config;
 	if (cfg.precision < GDN_CUDA_FP64 || cfg.precision > GDN_CUDA_BF16_STORE)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
-	if (cfg.elems_per_cta != 0 && cfg.elems_per_cta != 32 && cfg.elems_per_cta != 128)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: elems_per_cta must be 0 (auto), 32 or 128");
+	if (cfg.rk3_variant < 0 || cfg.rk3_variant > 2)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: rk3_variant must be 0 (auto), 1 or 2");
 	if (cfg.kin_sweep < 0 || cfg.kin_sweep > 2)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kin_sweep must be 0 (auto), 1 or 2");
 	for (int i = 0; i < n; i++) {
@@ -863,10 +865,10 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 	h->precision = cfg.precision;
 	h->refine_passes = cfg.refine_passes;
 	h->use_graph = cfg.use_graph;
-	// RK3 stage kernel: 32-element tiles with a warp per field, or 128-element
-	// tiles with a thread per element; 0 = timed at attach
-	h->rk3_variant = cfg.elems_per_cta == 128 ? 1 : 0;
-	h->rk3_autotune = cfg.elems_per_cta == 0;
+	// RK3 stage kernel compiled for fewer (1) or more (2) resident CTAs per
+	// SM; 0 = timed at attach
+	h->rk3_variant = cfg.rk3_variant == 2 ? 1 : 0;
+	h->rk3_autotune = cfg.rk3_variant == 0;
 	h->kin_mode = cfg.kin_sweep == 2 ? 2 : 1;
 	h->kin_autotune = cfg.kin_sweep == 0;
 	h->ninst = n;
@@ -977,10 +979,7 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, bt, RK_C[i], as<T>(h->btrace), h->stream));
 			nlaunch++;
 		}
-		if (h->rk3_variant == 1)
-			GDN_TRY(launch_rk3_stage_ept<T>(p, h->stream));
-		else
-			GDN_TRY(launch_rk3_stage<T>(p, h->stream));
+		GDN_TRY(launch_rk3_stage<T>(p, h->rk3_variant, h->stream));
 		nlaunch++;
 		cur = 1 - cur;
 	}
@@ -1332,9 +1331,9 @@ extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
 		const Data &d = h->hdata[i];
 		if (h->scheme == GDN_CUDA_SCHEME_RK3) {
 			if (h->precision == GDN_CUDA_FP64)
-				GDN_TRY(launch_init_rk3<double>(e2q, h->node, ne, d, as<double>(h->w[0]) + 60 * e0, s));
+				GDN_TRY(launch_init_rk3<double>(e2q, h->node, ne, e0, d, as<double>(h->w[0]), s));
 			else
-				GDN_TRY(launch_init_rk3<float>(e2q, h->node, ne, d, as<float>(h->w[0]) + 60 * e0, s));
+				GDN_TRY(launch_init_rk3<float>(e2q, h->node, ne, e0, d, as<float>(h->w[0]), s));
 		} else {
 			const int *pos = h->pos + e0 * h->nv;
 			if (sk == 0)
@@ -1348,7 +1347,7 @@ extern "C" int gdn_cuda_init(gdn_cuda_handle *h)
 	}
 	if (h->scheme == GDN_CUDA_SCHEME_RK3) {
 		h->cur = 0;
-		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * 32 * ((h->ne + 31) / 32) * h->ssize, s));
 	}
 	GDN_TRY(launch_set_time(h->batch(), 0.0, s));
 	h->launches++;
@@ -1372,17 +1371,15 @@ extern "C" int gdn_cuda_set_state(gdn_cuda_handle *h, const double *wn, double t
 		for (int i = 0; i < h->ninst; i++) {
 			const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
 			const double *src = wn + h->w_off[i];
-			if (h->precision == GDN_CUDA_FP64) {
-				GDN_CUDA_TRY(cudaMemcpyAsync(as<double>(h->w[0]) + 60 * e0, src, 60 * ne * sizeof(double),
-											 cudaMemcpyHostToDevice, s));
-			} else {
-				double *st = h->staging + h->w_off[i];
-				GDN_CUDA_TRY(cudaMemcpyAsync(st, src, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
-				GDN_TRY(launch_convert<float>(st, as<float>(h->w[0]) + 60 * e0, 60 * ne, s));
-				h->launches++;
-			}
+			double *st = h->staging + h->w_off[i];
+			GDN_CUDA_TRY(cudaMemcpyAsync(st, src, 60 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(launch_rk3_to_tiles<double>(st, as<double>(h->w[0]), e0, ne, s));
+			else
+				GDN_TRY(launch_rk3_to_tiles<float>(st, as<float>(h->w[0]), e0, ne, s));
+			h->launches++;
 		}
-		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * h->ne * h->ssize, s));
+		GDN_CUDA_TRY(cudaMemsetAsync(h->k2, 0, 60 * 32 * ((h->ne + 31) / 32) * h->ssize, s));
 	} else {
 		GDN_CUDA_TRY(cudaMemcpyAsync(h->staging, wn, h->w_off.back() * sizeof(double), cudaMemcpyHostToDevice, s));
 		for (int i = 0; i < h->ninst; i++) {
@@ -1412,14 +1409,12 @@ static int get_state_impl(gdn_cuda_handle *h, double *wn)
 			GDN_TRY(launch_boundary_dofs(h->bxyz + 18 * b0, nbf, h->hdata[i], h->ht_bdof[i], 0, h->km, neq,
 										 st + 60 * ne, s));
 			h->launches++;
-			if (h->precision == GDN_CUDA_FP64) {
-				GDN_CUDA_TRY(cudaMemcpyAsync(dst, as<double>(h->w[h->cur]) + 60 * e0, 60 * ne * sizeof(double),
-											 cudaMemcpyDeviceToHost, s));
-			} else {
-				GDN_TRY(launch_widen(as<float>(h->w[h->cur]) + 60 * e0, st, 60 * ne, s));
-				h->launches++;
-				GDN_CUDA_TRY(cudaMemcpyAsync(dst, st, 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
-			}
+			if (h->precision == GDN_CUDA_FP64)
+				GDN_TRY(launch_rk3_from_tiles<double>(as<double>(h->w[h->cur]), st, e0, ne, s));
+			else
+				GDN_TRY(launch_rk3_from_tiles<float>(as<float>(h->w[h->cur]), st, e0, ne, s));
+			h->launches++;
+			GDN_CUDA_TRY(cudaMemcpyAsync(dst, st, 60 * ne * sizeof(double), cudaMemcpyDeviceToHost, s));
 			if (nbf > 0)
 				GDN_CUDA_TRY(cudaMemcpyAsync(dst + 60 * ne, st + 60 * ne, 36 * nbf * sizeof(double),
 											 cudaMemcpyDeviceToHost, s));
@@ -1482,7 +1477,7 @@ static int error_l2_impl(gdn_cuda_handle *h, int i, double *err)
 	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
 	const int sk = kin ? kin_state_kind(h) : (h->precision == GDN_CUDA_FP64 ? 0 : 1);
 	const long long e0 = h->e_off[i], ne = h->e_off[i + 1] - e0;
-	const long long so = kin ? 0 : 60 * e0; // RK3 state offset; kinetic goes through pos
+	const long long te0 = kin ? 0 : e0; // RK3: tiled state indexed by global element; kinetic: through pos
 	const int *pos = kin ? h->pos + e0 * h->nv : nullptr;
 	const int *e2q = h->e2q + 10 * e0;
 	const double *geom = h->geom64 + 10 * e0;
@@ -1490,13 +1485,13 @@ static int error_l2_impl(gdn_cuda_handle *h, int i, double *err)
 	const double t = h->ht[i];
 	const Data &d = h->hdata[i];
 	if (sk == 0)
-		GDN_TRY(launch_error_l2<double>(as<double>(st) + so, kin, h->nv, pos, e2q, h->node, geom, ne, d, t,
+		GDN_TRY(launch_error_l2<double>(as<double>(st), kin, te0, h->nv, pos, e2q, h->node, geom, ne, d, t,
 										h->partial, h->nblk_err, h->result, s));
 	else if (sk == 1)
-		GDN_TRY(launch_error_l2<float>(as<float>(st) + so, kin, h->nv, pos, e2q, h->node, geom, ne, d, t, h->partial,
+		GDN_TRY(launch_error_l2<float>(as<float>(st), kin, te0, h->nv, pos, e2q, h->node, geom, ne, d, t, h->partial,
 									   h->nblk_err, h->result, s));
 	else
-		GDN_TRY(launch_error_l2<__nv_bfloat16>(as<__nv_bfloat16>(st) + so, kin, h->nv, pos, e2q, h->node, geom, ne, d,
+		GDN_TRY(launch_error_l2<__nv_bfloat16>(as<__nv_bfloat16>(st), kin, te0, h->nv, pos, e2q, h->node, geom, ne, d,
 											   t, h->partial, h->nblk_err, h->result, s));
 	h->launches += 2;
 	GDN_CUDA_TRY(cudaMemcpyAsync(h->host_result, h->result, 7 * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1539,11 +1534,14 @@ extern "C" int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode)
 	return GDN_CUDA_OK;
 }
 
-extern "C" int gdn_cuda_rk3_tile(gdn_cuda_handle *h, int *elems_per_cta)
+extern "C" int gdn_cuda_rk3_variant(gdn_cuda_handle *h, int *variant, int *min_ctas_per_sm)
 {
-	if (!h || !elems_per_cta)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "rk3_tile: bad arguments");
-	*elems_per_cta = h->scheme == GDN_CUDA_SCHEME_RK3 ? (h->rk3_variant == 1 ? 128 : 32) : 0;
+	if (!h || !variant)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "rk3_variant: bad arguments");
+	const bool rk = h->scheme == GDN_CUDA_SCHEME_RK3;
+	*variant = rk ? h->rk3_variant + 1 : 0;
+	if (min_ctas_per_sm)
+		*min_ctas_per_sm = rk ? rk3_min_blocks(h->precision == GDN_CUDA_FP64, h->rk3_variant) : 0;
 	return GDN_CUDA_OK;
 }
 

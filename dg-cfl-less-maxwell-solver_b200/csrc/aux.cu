@@ -79,10 +79,11 @@ __device__ __forceinline__ void node_xyz(const int *e2q, const double *node, lon
 	x[2] = node[3 * q + 2];
 }
 
-// dg_init_sol_macro, RK3 branch (src/dg/dg.c:32-59): w = w_exact(x, 0)
+// dg_init_sol_macro, RK3 branch (src/dg/dg.c:32-59): w = w_exact(x, 0) for
+// the elements e0 .. e0 + ne - 1 (e2q points at element e0), tiled layout
 template <typename S>
 __global__ void init_rk3_kernel(const int *__restrict__ e2q, const double *__restrict__ node, long long ne,
-								Data d, S *__restrict__ w)
+								long long e0, Data d, S *__restrict__ w)
 {
 	const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (t >= ne * 10)
@@ -93,19 +94,21 @@ __global__ void init_rk3_kernel(const int *__restrict__ e2q, const double *__res
 	node_xyz(e2q, node, e, i, x);
 	exact_w(d, x, 0.0, we);
 	for (int c = 0; c < 6; c++)
-		Store<S>::store(w + t * 6 + c, we[c]);
+		Store<S>::store(w + rk3_tix(e0 + e, i * 6 + c), we[c]);
 }
 
 template <typename S>
-int launch_init_rk3(const int *e2q, const double *node, long long ne, const Data &d, S *w, cudaStream_t s)
+int launch_init_rk3(const int *e2q, const double *node, long long ne, long long e0, const Data &d, S *w,
+					cudaStream_t s)
 {
-	init_rk3_kernel<S><<<(unsigned)((ne * 10 + 255) / 256), 256, 0, s>>>(e2q, node, ne, d, w);
+	init_rk3_kernel<S><<<(unsigned)((ne * 10 + 255) / 256), 256, 0, s>>>(e2q, node, ne, e0, d, w);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_init_rk3<double>(const int *, const double *, long long, const Data &, double *,
+template int launch_init_rk3<double>(const int *, const double *, long long, long long, const Data &, double *,
 									 cudaStream_t);
-template int launch_init_rk3<float>(const int *, const double *, long long, const Data &, float *, cudaStream_t);
+template int launch_init_rk3<float>(const int *, const double *, long long, long long, const Data &, float *,
+									cudaStream_t);
 
 // f_eq of the kinetic model: f_v = w / nv + feq_c A(v) w
 __device__ __forceinline__ void feq_component(const double w[6], const double *v, int nv, double feq_c,
@@ -292,7 +295,8 @@ template int launch_kin_pack<__nv_bfloat16>(const __nv_bfloat16 *, const int *, 
 // FP64 partial per block and field, in a fixed order; pass 2: one block sums
 // the partials in order.  Deterministic for a given launch shape.
 template <typename S>
-__global__ void error_partial_kernel(const S *__restrict__ state, int kinetic, int nv, const int *__restrict__ pos,
+__global__ void error_partial_kernel(const S *__restrict__ state, int kinetic, long long e0, int nv,
+									 const int *__restrict__ pos,
 									 const int *__restrict__ e2q, const double *__restrict__ node,
 									 const double *__restrict__ geom, long long ne, Data d, double t,
 									 double *__restrict__ partial)
@@ -309,7 +313,7 @@ __global__ void error_partial_kernel(const S *__restrict__ state, int kinetic, i
 		exact_w(d, x, t, we);
 		if (!kinetic) {
 			for (int c = 0; c < 6; c++)
-				wl[c] = (double)Store<S>::load(state + u * 6 + c);
+				wl[c] = (double)Store<S>::load(state + rk3_tix(e0 + e, i * 6 + c));
 		} else {
 			for (int c = 0; c < 6; c++) {
 				double s = 0.0;
@@ -365,23 +369,23 @@ __global__ void error_final_kernel(const double *__restrict__ partial, int nblk,
 }
 
 template <typename S>
-int launch_error_l2(const S *state, int kinetic, int nv, const int *pos, const int *e2q, const double *node,
-					const double *geom, long long ne, const Data &d, double t, double *partial, int nblk, double *out,
-					cudaStream_t s)
+int launch_error_l2(const S *state, int kinetic, long long e0, int nv, const int *pos, const int *e2q,
+					const double *node, const double *geom, long long ne, const Data &d, double t, double *partial,
+					int nblk, double *out, cudaStream_t s)
 {
-	error_partial_kernel<S><<<nblk, 256, 0, s>>>(state, kinetic, nv, pos, e2q, node, geom, ne, d, t, partial);
+	error_partial_kernel<S><<<nblk, 256, 0, s>>>(state, kinetic, e0, nv, pos, e2q, node, geom, ne, d, t, partial);
 	GDN_CUDA_TRY(cudaGetLastError());
 	error_final_kernel<<<1, 256, 0, s>>>(partial, nblk, out);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
-template int launch_error_l2<double>(const double *, int, int, const int *, const int *, const double *,
+template int launch_error_l2<double>(const double *, int, long long, int, const int *, const int *, const double *,
 									 const double *, long long, const Data &, double, double *, int, double *,
 									 cudaStream_t);
-template int launch_error_l2<float>(const float *, int, int, const int *, const int *, const double *,
+template int launch_error_l2<float>(const float *, int, long long, int, const int *, const int *, const double *,
 									const double *, long long, const Data &, double, double *, int, double *,
 									cudaStream_t);
-template int launch_error_l2<__nv_bfloat16>(const __nv_bfloat16 *, int, int, const int *, const int *,
+template int launch_error_l2<__nv_bfloat16>(const __nv_bfloat16 *, int, long long, int, const int *, const int *,
 											const double *, const double *, long long, const Data &, double, double *,
 											int, double *, cudaStream_t);
 

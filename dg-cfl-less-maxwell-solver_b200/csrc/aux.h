@@ -17,7 +17,8 @@ template <typename T>
 int launch_convert(const double *a, T *b, long long n, cudaStream_t s);
 int launch_widen(const float *a, double *b, long long n, cudaStream_t s);
 template <typename S>
-int launch_init_rk3(const int *e2q, const double *node, long long ne, const Data &d, S *w, cudaStream_t s);
+int launch_init_rk3(const int *e2q, const double *node, long long ne, long long e0, const Data &d, S *w,
+					cudaStream_t s);
 template <typename S>
 int launch_init_kin(const int *e2q, const double *node, long long ne, const Data &d, const KinModel &km,
 					const int *pos, S *f, cudaStream_t s);
@@ -27,8 +28,8 @@ template <typename S>
 int launch_kin_pack(const S *f, const int *pos, long long ne, int nv, long long neq, double *wn, int to_ref,
 					cudaStream_t s);
 template <typename S>
-int launch_error_l2(const S *state, int kinetic, int nv, const int *pos, const int *e2q, const double *node,
-					const double *geom, long long ne, const Data &d, double t, double *partial, int nblk, double *out,
-					cudaStream_t s);
+int launch_error_l2(const S *state, int kinetic, long long e0, int nv, const int *pos, const int *e2q,
+					const double *node, const double *geom, long long ne, const Data &d, double t, double *partial,
+					int nblk, double *out, cudaStream_t s);
 
 } // namespace gdn

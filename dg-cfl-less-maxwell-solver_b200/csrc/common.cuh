@@ -68,6 +68,13 @@ __device__ __forceinline__ const Tables<float> &tab<float>()
 	return c_tab_f;
 }
 
+// RK3 device layout: tiles of 32 elements, value-major inside a tile; value k
+// (= node * 6 + field) of element e.
+__host__ __device__ __forceinline__ long long rk3_tix(long long e, int k)
+{
+	return ((e >> 5) * 60 + k) * 32 + (e & 31);
+}
+
 // Analytic data (boundary values, initial data, error norm), FP64.
 struct Data {
 	int kind;

@@ -20,10 +20,10 @@ struct Batch {
 
 template <typename T>
 struct Rk3Params {
-	const T *w_in; // [ne][10][6] state read this stage
-	T *w_out; // [ne][10][6] state written this stage (ping-pong)
-	T *k2; // [ne][10][6] low-storage register, in place
-	const T *geom; // [ne][10] codtau (row-major 3x3), det
+	const T *w_in; // state read this stage, tiled (rk3_tix)
+	T *w_out; // state written this stage (ping-pong), tiled
+	T *k2; // low-storage register, in place, tiled
+	const T *geom; // codtau (row-major 3x3) and det, tiles of 32 elements x 10 values
 	const int *nb; // [ne][4] neighbour element, or -(boundary face + 1)
 	const int *perm; // [ne][4] neighbour local node of face node jj, 4 bits each
 	const T *btrace; // [nbf][6][6] boundary data at t_stage (boundary_trace_kernel)
@@ -39,14 +39,21 @@ struct Rk3Params {
 bool rk3_tables_sparse(const gdn_cuda_tables *t);
 bool rk3_tables_standard_faces(const gdn_cuda_tables *t);
 
+// variant 0 / 1: the stage kernel compiled for fewer / more resident CTAs per
+// SM (rk3_min_blocks), i.e. more / fewer registers per thread
 template <typename T>
-int launch_rk3_stage(const Rk3Params<T> &p, cudaStream_t s);
+int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s);
 template <typename T>
 int prepare_rk3();
+int rk3_min_blocks(int precision_fp64, int variant);
+// reference layout [e][node][field] (FP64, elements 0..ne-1) <-> tiled layout
+// at elements e0 .. e0 + ne - 1
 template <typename T>
-int launch_rk3_stage_ept(const Rk3Params<T> &p, cudaStream_t s);
+int launch_rk3_to_tiles(const double *src, T *dst, long long e0, long long ne, cudaStream_t s);
 template <typename T>
-int prepare_rk3_ept();
+int launch_rk3_from_tiles(const T *src, double *dst, long long e0, long long ne, cudaStream_t s);
+template <typename T>
+int launch_geom_to_tiles(const double *g, T *out, long long ne, cudaStream_t s);
 template <typename T>
 int launch_boundary_trace(const double *bxyz, long long nbf, const Batch &b, double c_stage, T *out, cudaStream_t s);
 int launch_set_time(const Batch &b, double value, cudaStream_t s);

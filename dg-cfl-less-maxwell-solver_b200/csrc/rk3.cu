@@ -19,19 +19,21 @@
 // (dg_update_boundary, dg.c:76-106), written by boundary_trace_kernel just
 // before the stage.
 //
-// Work decomposition (TE = 32 elements per CTA, 6 warps):
-//   A  16-byte coalesced loads of the tile (w, k2, geometry, neighbours) into
-//      shared memory, transposed to [value][element] with stride TE+1 so that
-//      lane = element is conflict-free everywhere below;
-//   B  flux: warp w evaluates face-node slots {w, w+6, w+12, w+18} of its 32
-//      elements (warp-uniform face / node);
-//   C  volume: warp c owns field c; the 10 nodal values stay in registers,
-//      r_k = D_k w_c with the tables as constant-bank FMA operands and the P2
-//      structural zeros removed at compile time; only the two physical
-//      derivatives the curl needs are written out (20 values);
-//   D  warp c assembles R_c = curl part + sum_faces S F_c, lifts with Minv
-//      (registers) and applies the RK update;
-//   E  16-byte coalesced stores.
+// Device layout: the state, k2 and the geometry are stored in tiles of 32
+// elements, value-major inside a tile (rk3_tix): value k of element e at
+// ((e / 32) * 60 + k) * 32 + e % 32.  A CTA owns one tile with 6 warps, lane =
+// element, so every per-element access of a warp is one coalesced 128-byte
+// (FP32) row and nothing is staged through shared memory:
+//   1  warp c (field c): the 10 nodal values of field c in registers (kept
+//      for the RK update), r_k = D_k w_c with the tables as constant-bank
+//      operands and the P2 structural zeros removed at compile time; only the
+//      two physical derivatives the curl needs go to shared memory;
+//   2  warp jj: the upwind flux at face node jj of the 4 faces (own traces from
+//      the tile, neighbour traces gathered from global, issued at kernel
+//      start so that phase 1 hides their latency) to shared memory;
+//   -- the one barrier --
+//   3  warp c: R_c = curl part + sum_faces S F_c, lift by Minv, RK update with
+//      k2 (prefetched before the barrier), coalesced stores.
 #include <cmath>
 
 #include "common.cuh"
@@ -152,112 +154,86 @@ __device__ __forceinline__ void lift_minv<float>(const Tables<float> &tb, const 
 	}
 }
 
-constexpr int kRk3Tile = 32; // elements per CTA
-constexpr int kRk3Threads = 192; // 6 warps
+constexpr int kRk3Threads = 192; // 6 warps, one 32-element tile
 
 template <typename T>
 struct Rk3Smem {
-	static constexpr int P = kRk3Tile + 1;
-	// sW 60, sK 60, sF 144, sX 120, sG 10 rows of P values; then 8 ints per element
-	static constexpr int rows = 60 + 60 + 144 + 120 + 10;
-	static constexpr int bytes = rows * P * (int)sizeof(T) + 8 * kRk3Tile * (int)sizeof(int);
+	static constexpr int P = 33;
+	// sX: (field*2 + which)*10 + node, 120 rows; sF: (face*6 + jj)*6 + c, 144 rows
+	static constexpr int bytes = (120 + 144) * P * (int)sizeof(T);
 };
 
-template <typename T, bool SPARSE>
-__global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
+// register cap (minimum resident CTAs per SM) of the two autotuned variants
+template <typename T>
+struct Rk3MinBlocks;
+template <>
+struct Rk3MinBlocks<float> {
+	static constexpr int lo = 4, hi = 5;
+};
+template <>
+struct Rk3MinBlocks<double> {
+	static constexpr int lo = 2, hi = 3;
+};
+
+template <typename T, bool SPARSE, int MINB>
+__global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<T> p)
 {
-	constexpr int TE = kRk3Tile, P = Rk3Smem<T>::P;
+	constexpr int P = Rk3Smem<T>::P;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	T *sW = reinterpret_cast<T *>(smem_raw); // [60][P]   value k = node*6 + field
-	T *sK = sW + 60 * P; // [60][P]
-	T *sF = sK + 60 * P; // [144][P]  (face*6 + jj)*6 + c
-	T *sX = sF + 144 * P; // [120][P]  (field*2 + which)*10 + node
-	T *sG = sX + 120 * P; // [10][P]   codtau row-major, det
-	int *sNb = reinterpret_cast<int *>(sG + 10 * P); // [TE][4]
-	int *sPm = sNb + 4 * TE; // [TE][4]
+	T *sX = reinterpret_cast<T *>(smem_raw); // [120][P]
+	T *sF = sX + 120 * P; // [144][P]
 
 	const Tables<T> &tb = tab<T>();
-	const int tid = threadIdx.x;
-	const int warp = tid >> 5, lane = tid & 31;
-	const long long e0 = (long long)blockIdx.x * TE;
-	const int nloc = (int)min((long long)TE, p.ne - e0);
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const long long tile = blockIdx.x;
+	const long long e = tile * 32 + lane;
+	const bool live = e < p.ne;
+	const T *Wt = p.w_in + tile * 60 * 32 + lane; // Wt[k * 32] = value k of element e
+	const T *Gt = p.geom + tile * 10 * 32 + lane;
 
-	// ---- A: stage the tile ----
-	{
-		constexpr int VPC = 16 / sizeof(T);
-		const int nch = nloc * 60 / VPC;
-		const uint4 *gw = reinterpret_cast<const uint4 *>(p.w_in + e0 * 60);
-		const uint4 *gk = reinterpret_cast<const uint4 *>(p.k2 + e0 * 60);
-		for (int ch = tid; ch < nch; ch += kRk3Threads) {
-			const int v0 = ch * VPC;
-			const int e = v0 / 60, k = v0 % 60;
-			const uint4 a = __ldg(gw + ch);
-			const T *av = reinterpret_cast<const T *>(&a);
-#pragma unroll
-			for (int q = 0; q < VPC; q++)
-				sW[(k + q) * P + e] = av[q];
-		}
-		if (!p.stage0) {
-			for (int ch = tid; ch < nch; ch += kRk3Threads) {
-				const int v0 = ch * VPC;
-				const int e = v0 / 60, k = v0 % 60;
-				const uint4 b = __ldcs(gk + ch);
-				const T *bv = reinterpret_cast<const T *>(&b);
-#pragma unroll
-				for (int q = 0; q < VPC; q++)
-					sK[(k + q) * P + e] = bv[q];
-			}
-		}
-		for (int v = tid; v < nloc * 10; v += kRk3Threads)
-			sG[(v % 10) * P + v / 10] = p.geom[e0 * 10 + v];
-		if (tid < nloc * 4) {
-			sNb[tid] = p.nb[e0 * 4 + tid];
-			sPm[tid] = p.perm[e0 * 4 + tid];
-		}
-	}
-	__syncthreads();
-
-	const int e = lane;
-	const bool live = e < nloc;
-
-	// out-of-tile neighbour traces (or boundary data at the stage time) of this
-	// thread's flux slots -- face node jj = warp of faces 0..3 -- issued now
-	// and consumed after the volume phase, which hides their latency
-	T pre[4][6];
+	int nbk[4] = {0, 0, 0, 0}, pmk[4] = {0, 0, 0, 0};
+	T cod[3][3], det = T(1);
+	// neighbour traces of this thread's flux slots (face node jj = warp of the
+	// 4 faces), issued first so that the volume phase hides their latency
+	T wR[4][6];
 	if (live) {
+		const int4 nb4 = __ldg(reinterpret_cast<const int4 *>(p.nb) + e);
+		const int4 pm4 = __ldg(reinterpret_cast<const int4 *>(p.perm) + e);
+		nbk[0] = nb4.x, nbk[1] = nb4.y, nbk[2] = nb4.z, nbk[3] = nb4.w;
+		pmk[0] = pm4.x, pmk[1] = pm4.y, pmk[2] = pm4.z, pmk[3] = pm4.w;
 		const int jj = warp;
 #pragma unroll
 		for (int f = 0; f < 4; f++) {
-			const int nbv = sNb[e * 4 + f];
-			const long long le = nbv - e0;
-			if (nbv < 0 || le < 0 || le >= nloc) {
-				const T *g = nbv >= 0 ? p.w_in + (long long)nbv * 60 + ((sPm[e * 4 + f] >> (4 * jj)) & 15) * 6
-									  : p.btrace + ((long long)(-nbv - 1) * 6 + jj) * 6;
+			const int nbv = nbk[f];
+			if (nbv >= 0) {
+				const int qn = (pmk[f] >> (4 * jj)) & 15;
+				const T *g = p.w_in + rk3_tix(nbv, qn * 6);
 #pragma unroll
 				for (int c = 0; c < 6; c++)
-					pre[f][c] = __ldg(g + c);
+					wR[f][c] = __ldg(g + c * 32);
 			} else {
+				const T *g = p.btrace + ((long long)(-nbv - 1) * 6 + jj) * 6;
 #pragma unroll
 				for (int c = 0; c < 6; c++)
-					pre[f][c] = T(0);
+					wR[f][c] = __ldg(g + c);
 			}
 		}
-	}
-
-	// ---- C: reference derivatives of field `warp`, two physical directions ----
-	const int c = warp; // field
-	const int a = c % 3;
-	if (live) {
-		T w[10];
-#pragma unroll
-		for (int j = 0; j < 10; j++)
-			w[j] = sW[(j * 6 + c) * P + e];
-		T cod[3][3];
 #pragma unroll
 		for (int r = 0; r < 3; r++)
 #pragma unroll
 			for (int q = 0; q < 3; q++)
-				cod[r][q] = sG[(3 * r + q) * P + e];
+				cod[r][q] = __ldg(Gt + (3 * r + q) * 32);
+		det = __ldg(Gt + 9 * 32);
+	}
+
+	// ---- 1: reference derivatives of field c = warp, two physical directions ----
+	const int c = warp;
+	const int a = c % 3;
+	T w[10];
+	if (live) {
+#pragma unroll
+		for (int j = 0; j < 10; j++)
+			w[j] = Wt[(j * 6 + c) * 32];
 		const int d1 = (a + 1) % 3, d2 = (a + 2) % 3;
 		T cd1[3], cd2[3];
 #pragma unroll
@@ -269,119 +245,83 @@ __global__ void __launch_bounds__(kRk3Threads) rk3_stage_kernel(Rk3Params<T> p)
 		ref_derivatives<T, SPARSE>(tb, w, r);
 #pragma unroll
 		for (int i = 0; i < 10; i++) {
-			sX[((c * 2 + 0) * 10 + i) * P + e] = cd1[0] * r[0][i] + cd1[1] * r[1][i] + cd1[2] * r[2][i];
-			sX[((c * 2 + 1) * 10 + i) * P + e] = cd2[0] * r[0][i] + cd2[1] * r[1][i] + cd2[2] * r[2][i];
+			sX[((c * 2 + 0) * 10 + i) * P + lane] = cd1[0] * r[0][i] + cd1[1] * r[1][i] + cd1[2] * r[2][i];
+			sX[((c * 2 + 1) * 10 + i) * P + lane] = cd2[0] * r[0][i] + cd2[1] * r[1][i] + cd2[2] * r[2][i];
 		}
 	}
 
-	// ---- B: upwind flux; warp w takes face node jj = w of the 4 faces ----
+	// ---- 2: upwind flux at face node jj = warp of the 4 faces ----
 	if (live) {
 		const int jj = warp;
-		T cod[3][3];
-#pragma unroll
-		for (int r = 0; r < 3; r++)
-#pragma unroll
-			for (int q = 0; q < 3; q++)
-				cod[r][q] = sG[(3 * r + q) * P + e];
 #pragma unroll
 		for (int f = 0; f < 4; f++) {
-			const int s = 6 * f + jj;
 			const int qo = tb.f2n[f][jj]; // warp-uniform: constant-cache broadcast
-			T wL[6], wR[6], vn[3], F[6];
+			T wL[6], vn[3], F[6];
 #pragma unroll
-			for (int c = 0; c < 6; c++)
-				wL[c] = sW[(qo * 6 + c) * P + e];
-			const int nbv = sNb[e * 4 + f];
-			const long long le = nbv - e0;
-			if (nbv >= 0 && le >= 0 && le < nloc) {
-				const int qn = (sPm[e * 4 + f] >> (4 * jj)) & 15;
-#pragma unroll
-				for (int c = 0; c < 6; c++)
-					wR[c] = sW[(qn * 6 + c) * P + (int)le];
-			} else {
-#pragma unroll
-				for (int c = 0; c < 6; c++)
-					wR[c] = pre[f][c];
-			}
+			for (int cc = 0; cc < 6; cc++)
+				wL[cc] = Wt[(qo * 6 + cc) * 32];
 			// own scaled outward normal codtau . n_ref(f): the reference
 			// normals are -e_0, -e_1, -e_2 and (1,1,1)/sqrt(3), face 3 scaled by
 			// sqrt(3) (simulation.c:377-395; checked at attach)
 #pragma unroll
 			for (int a2 = 0; a2 < 3; a2++)
 				vn[a2] = f < 3 ? -cod[a2][f] : (cod[a2][0] + cod[a2][1] + cod[a2][2]) * tb.n3scale;
-			upwind_flux<T>(wL, wR, vn, F);
+			upwind_flux<T>(wL, wR[f], vn, F);
 #pragma unroll
-			for (int c = 0; c < 6; c++)
-				sF[(s * 6 + c) * P + e] = F[c];
+			for (int cc = 0; cc < 6; cc++)
+				sF[((f * 6 + jj) * 6 + cc) * P + lane] = F[cc];
 		}
 	}
-
-	__syncthreads();
-
-	// ---- D: residual of field c, lift, RK update ----
-	if (live) {
-		// R_E,b = dH_{b+2}/dx_{b+1} - dH_{b+1}/dx_{b+2};  R_H,b = -(same with E)
-		const int X = c / 3, b = a;
-		const int fa = 3 * (1 - X) + (b + 2) % 3; // field whose "d2" slot holds d_{b+1}
-		const int fb = 3 * (1 - X) + (b + 1) % 3; // field whose "d1" slot holds d_{b+2}
-		const T sgn = X == 0 ? T(1) : T(-1);
-		T R[10];
+	T k2o[10];
+	T *Kt = p.k2 + tile * 60 * 32 + lane;
+	if (live && !p.stage0) {
 #pragma unroll
 		for (int i = 0; i < 10; i++)
-			R[i] = sgn * (sX[((fa * 2 + 1) * 10 + i) * P + e] - sX[((fb * 2 + 0) * 10 + i) * P + e]);
-#pragma unroll
-		for (int f = 0; f < 4; f++) {
-			T Fc[6];
-#pragma unroll
-			for (int jj = 0; jj < 6; jj++)
-				Fc[jj] = sF[((f * 6 + jj) * 6 + c) * P + e];
-#pragma unroll
-			for (int ii = 0; ii < 6; ii++) {
-				T acc = T(0);
-#pragma unroll
-				for (int jj = 0; jj < 6; jj++)
-					if (!SPARSE || (smask(ii) >> jj & 1))
-						acc += tb.S[ii][jj] * Fc[jj];
-				R[f2n(f, ii)] += acc;
-			}
-		}
-		const T inv_det = T(1) / sG[9 * P + e];
-		const T A = (T)p.A, B = (T)p.B;
-		const T dt = p.einst ? (T)p.dt_tab[p.einst[e0 + e]] : (T)p.dt;
-		T dwv[10];
-		lift_minv<T>(tb, R, dwv);
-#pragma unroll
-		for (int i = 0; i < 10; i++) {
-			const T dw = dwv[i];
-			const int o = (i * 6 + c) * P + e;
-			const T k2 = (p.stage0 ? T(0) : A * sK[o]) - dt * (dw * inv_det);
-			sK[o] = k2;
-			sW[o] = sW[o] + B * k2;
-		}
+			k2o[i] = Kt[(i * 6 + c) * 32];
 	}
+
 	__syncthreads();
 
-	// ---- E: write the tile back ----
-	{
-		constexpr int VPC = 16 / sizeof(T);
-		const int nch = nloc * 60 / VPC;
-		uint4 *gw = reinterpret_cast<uint4 *>(p.w_out + e0 * 60);
-		uint4 *gk = reinterpret_cast<uint4 *>(p.k2 + e0 * 60);
-		for (int ch = tid; ch < nch; ch += kRk3Threads) {
-			const int v0 = ch * VPC;
-			const int ee = v0 / 60, k = v0 % 60;
-			uint4 av, bv;
-			T *ap = reinterpret_cast<T *>(&av);
-			T *bp = reinterpret_cast<T *>(&bv);
+	// ---- 3: residual of field c, lift, RK update ----
+	if (!live)
+		return;
+	// R_E,b = dH_{b+2}/dx_{b+1} - dH_{b+1}/dx_{b+2};  R_H,b = -(same with E)
+	const int X = c / 3, b = a;
+	const int fa = 3 * (1 - X) + (b + 2) % 3; // field whose "d2" slot holds d_{b+1}
+	const int fb = 3 * (1 - X) + (b + 1) % 3; // field whose "d1" slot holds d_{b+2}
+	const T sgn = X == 0 ? T(1) : T(-1);
+	T R[10];
 #pragma unroll
-			for (int q = 0; q < VPC; q++) {
-				ap[q] = sW[(k + q) * P + ee];
-				bp[q] = sK[(k + q) * P + ee];
-			}
-			__stcs(gw + ch, av);
-			if (p.write_k2)
-				__stcs(gk + ch, bv);
+	for (int i = 0; i < 10; i++)
+		R[i] = sgn * (sX[((fa * 2 + 1) * 10 + i) * P + lane] - sX[((fb * 2 + 0) * 10 + i) * P + lane]);
+#pragma unroll
+	for (int f = 0; f < 4; f++) {
+		T Fc[6];
+#pragma unroll
+		for (int jj = 0; jj < 6; jj++)
+			Fc[jj] = sF[((f * 6 + jj) * 6 + c) * P + lane];
+#pragma unroll
+		for (int ii = 0; ii < 6; ii++) {
+			T acc = T(0);
+#pragma unroll
+			for (int jj = 0; jj < 6; jj++)
+				if (!SPARSE || (smask(ii) >> jj & 1))
+					acc += tb.S[ii][jj] * Fc[jj];
+			R[f2n(f, ii)] += acc;
 		}
+	}
+	const T inv_det = T(1) / det;
+	const T A = (T)p.A, B = (T)p.B;
+	const T dt = p.einst ? (T)p.dt_tab[p.einst[e]] : (T)p.dt;
+	T dwv[10];
+	lift_minv<T>(tb, R, dwv);
+	T *Wo = p.w_out + tile * 60 * 32 + lane;
+#pragma unroll
+	for (int i = 0; i < 10; i++) {
+		const T k2 = (p.stage0 ? T(0) : A * k2o[i]) - dt * (dwv[i] * inv_det);
+		Wo[(i * 6 + c) * 32] = w[i] + B * k2;
+		if (p.write_k2)
+			Kt[(i * 6 + c) * 32] = k2;
 	}
 }
 
@@ -420,28 +360,116 @@ bool rk3_tables_standard_faces(const gdn_cuda_tables *t)
 template <typename T>
 int prepare_rk3()
 {
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	constexpr int lo = Rk3MinBlocks<T>::lo, hi = Rk3MinBlocks<T>::hi;
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, lo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, lo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+									  Rk3Smem<T>::bytes));
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, hi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+									  Rk3Smem<T>::bytes));
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, hi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 									  Rk3Smem<T>::bytes));
 	return GDN_CUDA_OK;
 }
 
+// variant 0: register cap for Rk3MinBlocks::lo CTAs per SM, 1: for ::hi
 template <typename T>
-int launch_rk3_stage(const Rk3Params<T> &p, cudaStream_t s)
+int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s)
 {
-	const long long nblk = (p.ne + kRk3Tile - 1) / kRk3Tile;
-	if (p.sparse)
-		rk3_stage_kernel<T, true><<<(unsigned)nblk, kRk3Threads, Rk3Smem<T>::bytes, s>>>(p);
-	else
-		rk3_stage_kernel<T, false><<<(unsigned)nblk, kRk3Threads, Rk3Smem<T>::bytes, s>>>(p);
+	constexpr int lo = Rk3MinBlocks<T>::lo, hi = Rk3MinBlocks<T>::hi;
+	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
+	const int sm = Rk3Smem<T>::bytes;
+	if (variant == 0) {
+		if (p.sparse)
+			rk3_stage_kernel<T, true, lo><<<nblk, kRk3Threads, sm, s>>>(p);
+		else
+			rk3_stage_kernel<T, false, lo><<<nblk, kRk3Threads, sm, s>>>(p);
+	} else {
+		if (p.sparse)
+			rk3_stage_kernel<T, true, hi><<<nblk, kRk3Threads, sm, s>>>(p);
+		else
+			rk3_stage_kernel<T, false, hi><<<nblk, kRk3Threads, sm, s>>>(p);
+	}
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+
+int rk3_min_blocks(int precision_fp64, int variant)
+{
+	if (precision_fp64)
+		return variant == 0 ? Rk3MinBlocks<double>::lo : Rk3MinBlocks<double>::hi;
+	return variant == 0 ? Rk3MinBlocks<float>::lo : Rk3MinBlocks<float>::hi;
+}
+
+// reference layout [e][node i][field c] (FP64, local elements 0..ne-1) <->
+// tiles (global elements e0 + e)
+template <typename T>
+__global__ void rk3_to_tiles_kernel(const double *__restrict__ src, T *__restrict__ dst, long long e0, long long ne)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= ne * 60)
+		return;
+	const long long e = u / 60;
+	const int k = (int)(u % 60);
+	dst[rk3_tix(e0 + e, k)] = (T)src[u];
+}
+template <typename T>
+__global__ void rk3_from_tiles_kernel(const T *__restrict__ src, double *__restrict__ dst, long long e0, long long ne)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= ne * 60)
+		return;
+	const long long e = u / 60;
+	const int k = (int)(u % 60);
+	dst[u] = (double)src[rk3_tix(e0 + e, k)];
+}
+// geometry [e][10] FP64 -> tiles of T
+template <typename T>
+__global__ void geom_to_tiles_kernel(const double *__restrict__ g, T *__restrict__ out, long long ne)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= ne * 10)
+		return;
+	const long long e = u / 10;
+	const int q = (int)(u % 10);
+	out[((e >> 5) * 10 + q) * 32 + (e & 31)] = (T)g[u];
+}
+
+template <typename T>
+int launch_rk3_to_tiles(const double *src, T *dst, long long e0, long long ne, cudaStream_t s)
+{
+	if (ne <= 0)
+		return GDN_CUDA_OK;
+	rk3_to_tiles_kernel<T><<<(unsigned)((ne * 60 + 255) / 256), 256, 0, s>>>(src, dst, e0, ne);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+template <typename T>
+int launch_rk3_from_tiles(const T *src, double *dst, long long e0, long long ne, cudaStream_t s)
+{
+	if (ne <= 0)
+		return GDN_CUDA_OK;
+	rk3_from_tiles_kernel<T><<<(unsigned)((ne * 60 + 255) / 256), 256, 0, s>>>(src, dst, e0, ne);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+template <typename T>
+int launch_geom_to_tiles(const double *g, T *out, long long ne, cudaStream_t s)
+{
+	geom_to_tiles_kernel<T><<<(unsigned)((ne * 10 + 255) / 256), 256, 0, s>>>(g, out, ne);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }
 
 template int prepare_rk3<double>();
 template int prepare_rk3<float>();
-template int launch_rk3_stage<double>(const Rk3Params<double> &, cudaStream_t);
-template int launch_rk3_stage<float>(const Rk3Params<float> &, cudaStream_t);
+template int launch_rk3_stage<double>(const Rk3Params<double> &, int, cudaStream_t);
+template int launch_rk3_stage<float>(const Rk3Params<float> &, int, cudaStream_t);
+template int launch_rk3_to_tiles<double>(const double *, double *, long long, long long, cudaStream_t);
+template int launch_rk3_to_tiles<float>(const double *, float *, long long, long long, cudaStream_t);
+template int launch_rk3_from_tiles<double>(const double *, double *, long long, long long, cudaStream_t);
+template int launch_rk3_from_tiles<float>(const float *, double *, long long, long long, cudaStream_t);
+template int launch_geom_to_tiles<double>(const double *, double *, long long, cudaStream_t);
+template int launch_geom_to_tiles<float>(const double *, float *, long long, cudaStream_t);
 
 } // namespace gdn

@@ -3,7 +3,6 @@
 // translation unit shares them without relocatable device code.
 #include "aux.cu"
 #include "rk3.cu"
-#include "rk3_ept.cu"
 #include "kinetic.cu"
 #include "api.cu"
 #include "noalloc.cu"

@@ -111,10 +111,11 @@ typedef struct gdn_cuda_config {
 	int precision;
 	int refine_passes; /* GDN_CUDA_FP32_REFINE: FP64-residual correction passes
 	                      per transport solve, 0 to 4 */
-	int elems_per_cta; /* RK3 stage kernel: 32 (a warp per field of 32-element
-	                      tiles), 128 (a thread per element), 0 = the faster
-	                      of the two, timed at attach and cached per
-	                      (precision, mesh-size bucket) */
+	int rk3_variant; /* RK3 stage kernel (32-element tiles, a warp per field):
+	                    1 = compiled for fewer resident CTAs per SM (more
+	                    registers per thread), 2 = for more resident CTAs,
+	                    0 = the faster of the two, timed at attach and cached
+	                    per (precision, mesh-size bucket) */
 	int use_graph; /* capture step loops as CUDA graphs (1 = yes) */
 	int device; /* CUDA device ordinal */
 	int kin_sweep; /* kinetic transport solve: 1 = a launch per sweep level,
@@ -235,8 +236,10 @@ int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
 int gdn_cuda_num_instances(gdn_cuda_handle *h, int *ninst);
 /* kinetic: the sweep mode in use (1 or 2, see kin_sweep; 0 for RK3) */
 int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode);
-/* RK3: the stage kernel's element tile in use (32 or 128; 0 for kinetic) */
-int gdn_cuda_rk3_tile(gdn_cuda_handle *h, int *elems_per_cta);
+/* RK3: the stage-kernel variant in use (1 or 2, see rk3_variant; 0 for the
+ * kinetic scheme) and the resident CTAs per SM it was compiled for (may be
+ * NULL) */
+int gdn_cuda_rk3_variant(gdn_cuda_handle *h, int *variant, int *min_ctas_per_sm);
 /* instance i of a batch: its time, element count and the offset / length of
  * its reference-layout state in the batch state vector (any output may be
  * NULL) */

@@ -37,9 +37,9 @@ def _instances(scheme):
 def test_batch_equals_single_instance_solves(scheme, precision):
     meshes, datas, dts = _instances(scheme)
     steps = 5
-    # one RK3 tile for both runs: the autotuner may pick different stage
-    # kernels for the batch and the single meshes
-    b = capi.BatchSolver(meshes, datas, dts, scheme=scheme, precision=precision, elems_per_cta=32)
+    # one RK3 stage-kernel variant for both runs: the autotuner may pick
+    # different ones for the batch and the single meshes
+    b = capi.BatchSolver(meshes, datas, dts, scheme=scheme, precision=precision, rk3_variant=1)
     assert b.ninst == 3
     wn, t0, _ = b.solve(steps)
     errs = b.error_l2_batch()
@@ -47,7 +47,7 @@ def test_batch_equals_single_instance_solves(scheme, precision):
     times = [b.instance_info(i)[0] for i in range(3)]
     b.close()
     for i in range(3):
-        s = capi.Solver(meshes[i], scheme, datas[i], dts[i], precision=precision, elems_per_cta=32)
+        s = capi.Solver(meshes[i], scheme, datas[i], dts[i], precision=precision, rk3_variant=1)
         wi, ti, _ = s.solve(steps)
         ei = s.error_l2()
         s.close()
