@@ -81,44 +81,6 @@ __device__ __forceinline__ void ref_derivatives(const Tables<T> &tb, const T w[1
 		}
 }
 
-// FP32: the same sums with Blackwell's packed FP32x2 FMA, pairing
-// (r0[i], r1[i]) and (r2[2m], r2[2m+1]); coefficient pairs are stored
-// adjacent in constant memory (Tables<float>::D01, D2p).
-template <>
-__device__ __forceinline__ void ref_derivatives<float, true>(const Tables<float> &tb, const float w[10],
-															 float r[3][10])
-{
-	float2 p01[10], p2[5];
-#pragma unroll
-	for (int i = 0; i < 10; i++)
-		p01[i] = make_float2(0.f, 0.f);
-#pragma unroll
-	for (int m = 0; m < 5; m++)
-		p2[m] = make_float2(0.f, 0.f);
-#pragma unroll
-	for (int j = 0; j < 10; j++) {
-		const float2 wd = make_float2(w[j], w[j]);
-#pragma unroll
-		for (int i = 0; i < 10; i++)
-			if ((dmask(0, i) | dmask(1, i)) >> j & 1)
-				p01[i] = __ffma2_rn(tb.D01[i][j], wd, p01[i]);
-#pragma unroll
-		for (int m = 0; m < 5; m++)
-			if ((dmask(2, 2 * m) | dmask(2, 2 * m + 1)) >> j & 1)
-				p2[m] = __ffma2_rn(tb.D2p[m][j], wd, p2[m]);
-	}
-#pragma unroll
-	for (int i = 0; i < 10; i++) {
-		r[0][i] = p01[i].x;
-		r[1][i] = p01[i].y;
-	}
-#pragma unroll
-	for (int m = 0; m < 5; m++) {
-		r[2][2 * m] = p2[m].x;
-		r[2][2 * m + 1] = p2[m].y;
-	}
-}
-
 // dw = Minv R (dense 10 x 10)
 template <typename T>
 __device__ __forceinline__ void lift_minv(const Tables<T> &tb, const T R[10], T dw[10])
@@ -163,19 +125,23 @@ struct Rk3Smem {
 	static constexpr int bytes = (120 + 144) * P * (int)sizeof(T);
 };
 
-// register cap (minimum resident CTAs per SM) of the two autotuned variants
+// The two autotuned variants: register cap (minimum resident CTAs per SM) and
+// whether the neighbour traces are prefetched at kernel start (24 live values
+// through the volume phase) or loaded in the flux phase.
 template <typename T>
-struct Rk3MinBlocks;
+struct Rk3Variants;
 template <>
-struct Rk3MinBlocks<float> {
+struct Rk3Variants<float> {
 	static constexpr int lo = 4, hi = 5;
+	static constexpr bool pf_lo = true, pf_hi = true;
 };
 template <>
-struct Rk3MinBlocks<double> {
+struct Rk3Variants<double> {
 	static constexpr int lo = 2, hi = 3;
+	static constexpr bool pf_lo = true, pf_hi = false;
 };
 
-template <typename T, bool SPARSE, int MINB>
+template <typename T, bool SPARSE, int MINB, bool PF>
 __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<T> p)
 {
 	constexpr int P = Rk3Smem<T>::P;
@@ -193,30 +159,34 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 
 	int nbk[4] = {0, 0, 0, 0}, pmk[4] = {0, 0, 0, 0};
 	T cod[3][3], det = T(1);
-	// neighbour traces of this thread's flux slots (face node jj = warp of the
-	// 4 faces), issued first so that the volume phase hides their latency
-	T wR[4][6];
+	// neighbour traces of this thread's flux slot (face node jj = warp) of face f
+	auto load_wR = [&](int f, T out[6]) {
+		const int nbv = nbk[f];
+		const int jj = warp;
+		if (nbv >= 0) {
+			const int qn = (pmk[f] >> (4 * jj)) & 15;
+			const T *g = p.w_in + rk3_tix(nbv, qn * 6);
+#pragma unroll
+			for (int c = 0; c < 6; c++)
+				out[c] = __ldg(g + c * 32);
+		} else {
+			const T *g = p.btrace + ((long long)(-nbv - 1) * 6 + jj) * 6;
+#pragma unroll
+			for (int c = 0; c < 6; c++)
+				out[c] = __ldg(g + c);
+		}
+	};
+	// with PF they are issued first so that the volume phase hides their latency
+	T wR[PF ? 4 : 1][6];
 	if (live) {
 		const int4 nb4 = __ldg(reinterpret_cast<const int4 *>(p.nb) + e);
 		const int4 pm4 = __ldg(reinterpret_cast<const int4 *>(p.perm) + e);
 		nbk[0] = nb4.x, nbk[1] = nb4.y, nbk[2] = nb4.z, nbk[3] = nb4.w;
 		pmk[0] = pm4.x, pmk[1] = pm4.y, pmk[2] = pm4.z, pmk[3] = pm4.w;
-		const int jj = warp;
+		if (PF) {
 #pragma unroll
-		for (int f = 0; f < 4; f++) {
-			const int nbv = nbk[f];
-			if (nbv >= 0) {
-				const int qn = (pmk[f] >> (4 * jj)) & 15;
-				const T *g = p.w_in + rk3_tix(nbv, qn * 6);
-#pragma unroll
-				for (int c = 0; c < 6; c++)
-					wR[f][c] = __ldg(g + c * 32);
-			} else {
-				const T *g = p.btrace + ((long long)(-nbv - 1) * 6 + jj) * 6;
-#pragma unroll
-				for (int c = 0; c < 6; c++)
-					wR[f][c] = __ldg(g + c);
-			}
+			for (int f = 0; f < 4; f++)
+				load_wR(f, wR[PF ? f : 0]);
 		}
 #pragma unroll
 		for (int r = 0; r < 3; r++)
@@ -266,7 +236,9 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 #pragma unroll
 			for (int a2 = 0; a2 < 3; a2++)
 				vn[a2] = f < 3 ? -cod[a2][f] : (cod[a2][0] + cod[a2][1] + cod[a2][2]) * tb.n3scale;
-			upwind_flux<T>(wL, wR[f], vn, F);
+			if (!PF)
+				load_wR(f, wR[0]);
+			upwind_flux<T>(wL, wR[PF ? f : 0], vn, F);
 #pragma unroll
 			for (int cc = 0; cc < 6; cc++)
 				sF[((f * 6 + jj) * 6 + cc) * P + lane] = F[cc];
@@ -310,15 +282,15 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 			R[f2n(f, ii)] += acc;
 		}
 	}
-	const T inv_det = T(1) / det;
 	const T A = (T)p.A, B = (T)p.B;
 	const T dt = p.einst ? (T)p.dt_tab[p.einst[e]] : (T)p.dt;
+	const T scale = dt / det;
 	T dwv[10];
 	lift_minv<T>(tb, R, dwv);
 	T *Wo = p.w_out + tile * 60 * 32 + lane;
 #pragma unroll
 	for (int i = 0; i < 10; i++) {
-		const T k2 = (p.stage0 ? T(0) : A * k2o[i]) - dt * (dwv[i] * inv_det);
+		const T k2 = p.stage0 ? -(scale * dwv[i]) : A * k2o[i] - scale * dwv[i];
 		Wo[(i * 6 + c) * 32] = w[i] + B * k2;
 		if (p.write_k2)
 			Kt[(i * 6 + c) * 32] = k2;
@@ -360,15 +332,15 @@ bool rk3_tables_standard_faces(const gdn_cuda_tables *t)
 template <typename T>
 int prepare_rk3()
 {
-	constexpr int lo = Rk3MinBlocks<T>::lo, hi = Rk3MinBlocks<T>::hi;
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, lo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-									  Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, lo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-									  Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, hi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-									  Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, hi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-									  Rk3Smem<T>::bytes));
+	typedef Rk3Variants<T> V;
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, V::lo, V::pf_lo>,
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, V::lo, V::pf_lo>,
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, V::hi, V::pf_hi>,
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, V::hi, V::pf_hi>,
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
 	return GDN_CUDA_OK;
 }
 
@@ -376,19 +348,19 @@ int prepare_rk3()
 template <typename T>
 int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s)
 {
-	constexpr int lo = Rk3MinBlocks<T>::lo, hi = Rk3MinBlocks<T>::hi;
+	typedef Rk3Variants<T> V;
 	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
 	const int sm = Rk3Smem<T>::bytes;
 	if (variant == 0) {
 		if (p.sparse)
-			rk3_stage_kernel<T, true, lo><<<nblk, kRk3Threads, sm, s>>>(p);
+			rk3_stage_kernel<T, true, V::lo, V::pf_lo><<<nblk, kRk3Threads, sm, s>>>(p);
 		else
-			rk3_stage_kernel<T, false, lo><<<nblk, kRk3Threads, sm, s>>>(p);
+			rk3_stage_kernel<T, false, V::lo, V::pf_lo><<<nblk, kRk3Threads, sm, s>>>(p);
 	} else {
 		if (p.sparse)
-			rk3_stage_kernel<T, true, hi><<<nblk, kRk3Threads, sm, s>>>(p);
+			rk3_stage_kernel<T, true, V::hi, V::pf_hi><<<nblk, kRk3Threads, sm, s>>>(p);
 		else
-			rk3_stage_kernel<T, false, hi><<<nblk, kRk3Threads, sm, s>>>(p);
+			rk3_stage_kernel<T, false, V::hi, V::pf_hi><<<nblk, kRk3Threads, sm, s>>>(p);
 	}
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
@@ -397,8 +369,8 @@ int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s)
 int rk3_min_blocks(int precision_fp64, int variant)
 {
 	if (precision_fp64)
-		return variant == 0 ? Rk3MinBlocks<double>::lo : Rk3MinBlocks<double>::hi;
-	return variant == 0 ? Rk3MinBlocks<float>::lo : Rk3MinBlocks<float>::hi;
+		return variant == 0 ? Rk3Variants<double>::lo : Rk3Variants<double>::hi;
+	return variant == 0 ? Rk3Variants<float>::lo : Rk3Variants<float>::hi;
 }
 
 // reference layout [e][node i][field c] (FP64, local elements 0..ne-1) <->
