@@ -18,6 +18,7 @@ OK = 0
 ERR_CUDA, ERR_INVALID, ERR_UNSUPPORTED, ERR_CYCLE, ERR_OOM, ERR_TIMEOUT, ERR_MESH = 1, 2, 3, 4, 5, 6, 7
 DATA_PLANE, DATA_CAVITY = 0, 1
 SCHEME_RK3, SCHEME_KINETIC = 0, 1
+BC_UPWIND, BC_METAL = 0, 1
 FP64, FP32, FP32_REFINE, BF16_STORE = 0, 1, 2, 3
 
 # d3q4 / d3q6 velocity sets (src/models/d3q4.c:17-24, src/models/d3q6.c:18-24)
@@ -56,7 +57,8 @@ class Data(C.Structure):
 
 class Model(C.Structure):
     _fields_ = [("scheme", C.c_int), ("nb_w", C.c_int), ("nb_v", C.c_int), ("lambda_", C.c_double),
-                ("omega", C.c_double), ("vi", C.POINTER(C.c_double)), ("theta", C.c_double)]
+                ("omega", C.c_double), ("vi", C.POINTER(C.c_double)), ("theta", C.c_double),
+                ("boundary_flux", C.c_int)]
 
 
 class Instance(C.Structure):
@@ -242,31 +244,31 @@ class Solver:
 
     def __init__(self, mesh: MeshArrays, scheme=SCHEME_RK3, data: Data = None, dt: float = None,
                  precision=FP64, nb_v=4, tables: Tables = None, device=0, use_graph=1,
-                 refine_passes=1, theta=0.5, rk3_variant=0, kin_sweep=0):
+                 refine_passes=1, theta=0.5, rk3_variant=0, kin_sweep=0, boundary_flux=BC_UPWIND):
         self.L = lib()
         self.h = C.c_void_p()
         self.mesh = mesh
         self.scheme = scheme
         self.tables = tables if tables is not None else t10_tables()
         self.data = data if data is not None else plane_data()
-        model = self._model(scheme, nb_v, theta)
+        model = self._model(scheme, nb_v, theta, boundary_flux)
         cfg = Config(precision, refine_passes, rk3_variant, use_graph, device, kin_sweep)
         check(self.L.gdn_cuda_attach(C.byref(mesh.struct), C.byref(self.tables), C.byref(model),
                                      C.byref(self.data), C.byref(cfg), float(dt), C.byref(self.h)))
         self.dt = float(dt)
 
-    def _model(self, scheme, nb_v, theta):
+    def _model(self, scheme, nb_v, theta, boundary_flux=BC_UPWIND):
         """The gdn_model descriptor of the scheme (vi kept alive on self)."""
         if scheme == SCHEME_RK3:
             self._vi = np.zeros(3, np.float64)
             self.m = 6
-            model = Model(SCHEME_RK3, 6, 0, 1.0, 0.0, _dp(self._vi), 0.5)
+            model = Model(SCHEME_RK3, 6, 0, 1.0, 0.0, _dp(self._vi), 0.5, boundary_flux)
         else:
             lam = D3Q4_LAMBDA if nb_v == 4 else D3Q6_LAMBDA
             base = D3Q4_VI if nb_v == 4 else D3Q6_VI
             self._vi = np.ascontiguousarray((base * lam).ravel())
             self.m = 6 * nb_v
-            model = Model(SCHEME_KINETIC, 6, nb_v, lam, RELAX_OMEGA, _dp(self._vi), theta)
+            model = Model(SCHEME_KINETIC, 6, nb_v, lam, RELAX_OMEGA, _dp(self._vi), theta, boundary_flux)
         self.nb_v = nb_v
         self._model_struct = model
         return model

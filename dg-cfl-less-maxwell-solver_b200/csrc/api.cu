@@ -74,6 +74,7 @@ struct gdn_cuda_handle {
 	long long launches = 0;
 	int ssize = 8; // bytes per stored state value
 	int rk3_sparse = 1; // tables follow the P2 structural-zero pattern
+	int bc_metal = 0; // RK3 boundary faces take the metal flux
 	// device arrays
 	std::vector<DevBuf> bufs;
 	int *e2q = nullptr;
@@ -474,6 +475,7 @@ static int autotune_rk3(gdn_cuda_handle *h)
 	p.stage0 = 0;
 	p.write_k2 = 1;
 	p.sparse = h->rk3_sparse;
+	p.bc_metal = h->bc_metal;
 	cudaEvent_t ev[2];
 	GDN_CUDA_TRY(cudaEventCreate(&ev[0]));
 	GDN_CUDA_TRY(cudaEventCreate(&ev[1]));
@@ -731,6 +733,11 @@ static int validate_model(const gdn_cuda_model *model, const gdn_cuda_config &cf
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: unknown scheme");
 	if (model->scheme == GDN_CUDA_SCHEME_RK3 && cfg.precision > GDN_CUDA_FP32)
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: RK3 supports FP64 and FP32");
+	if (model->boundary_flux != GDN_CUDA_BC_UPWIND && model->boundary_flux != GDN_CUDA_BC_METAL)
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: unknown boundary flux");
+	if (model->scheme == GDN_CUDA_SCHEME_KINETIC && model->boundary_flux != GDN_CUDA_BC_UPWIND)
+		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED,
+							 "attach: the kinetic scheme imposes f_eq of the data on boundaries (upwind only)");
 	if (model->scheme == GDN_CUDA_SCHEME_KINETIC) {
 		if (model->nb_v != 4 && model->nb_v != 6)
 			return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: kinetic sets d3q4 (4) or d3q6 (6) only");
@@ -746,7 +753,7 @@ static int validate_model(const gdn_cuda_model *model, const gdn_cuda_config &cf
 // whole velocity model (one relaxation kernel serves them all)
 static bool same_model(const gdn_cuda_model *a, const gdn_cuda_model *b)
 {
-	if (a->scheme != b->scheme)
+	if (a->scheme != b->scheme || a->boundary_flux != b->boundary_flux)
 		return false;
 	if (a->scheme == GDN_CUDA_SCHEME_RK3)
 		return true;
@@ -881,6 +888,7 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 	h->theta = model->theta > 0 ? model->theta : 0.5;
 	h->omega = model->omega;
 	h->lambda = model->lambda;
+	h->bc_metal = model->boundary_flux == GDN_CUDA_BC_METAL;
 	h->ssize = cfg.precision == GDN_CUDA_FP64 ? 8 : 4;
 	if (h->scheme == GDN_CUDA_SCHEME_KINETIC) {
 		h->nv = model->nb_v;
@@ -975,6 +983,7 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 		p.stage0 = i == 0;
 		p.write_k2 = i < 2;
 		p.sparse = h->rk3_sparse;
+		p.bc_metal = h->bc_metal;
 		if (h->nbf > 0) {
 			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, bt, RK_C[i], as<T>(h->btrace), h->stream));
 			nlaunch++;

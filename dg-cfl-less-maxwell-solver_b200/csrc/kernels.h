@@ -34,6 +34,7 @@ struct Rk3Params {
 	int stage0; // k2 = -dt dw (no k2 read)
 	int write_k2; // 0 on the last stage: k2 is dead until the next stage 0
 	int sparse; // tables follow the P2 structural-zero pattern
+	int bc_metal; // boundary faces take the metal flux (-n x H_L, 0)
 };
 
 bool rk3_tables_sparse(const gdn_cuda_tables *t);

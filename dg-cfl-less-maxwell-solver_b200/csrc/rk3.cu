@@ -169,7 +169,7 @@ __device__ __forceinline__ void upwind_flux_h(const T wL[6], const T wR[6], cons
 	F[5] = (h[0] * sE[1] - h[1] * sE[0]) + r2 * (n[2] * nH - nn * dH[2]);
 }
 
-template <typename T, bool SPARSE, int MINB, bool PF>
+template <typename T, bool SPARSE, int MINB, bool PF, bool METAL>
 __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<T> p)
 {
 	constexpr int P = Rk3Smem<T>::P;
@@ -266,7 +266,15 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 				vn[a2] = f < 3 ? -cod[a2][f] : (cod[a2][0] + cod[a2][1] + cod[a2][2]) * tb.n3scale;
 			if (!PF)
 				load_wR(f, wR[0]);
-			upwind_flux_h<T>(wL, wR[PF ? f : 0], vn, F);
+			if (METAL && nbk[f] < 0) {
+				// maxwell_num_flux_boundary_metal (maxwell.c:205-223)
+				F[0] = vn[2] * wL[4] - vn[1] * wL[5];
+				F[1] = -vn[2] * wL[3] + vn[0] * wL[5];
+				F[2] = -vn[0] * wL[4] + vn[1] * wL[3];
+				F[3] = F[4] = F[5] = T(0);
+			} else {
+				upwind_flux_h<T>(wL, wR[PF ? f : 0], vn, F);
+			}
 #pragma unroll
 			for (int cc = 0; cc < 6; cc++)
 				sF[((f * 6 + jj) * 6 + cc) * P + lane] = F[cc];
@@ -357,38 +365,60 @@ bool rk3_tables_standard_faces(const gdn_cuda_tables *t)
 	return true;
 }
 
+#define GDN_RK3_TRY(expr)                                                                                         \
+	do {                                                                                                           \
+		int _rc = (expr);                                                                                          \
+		if (_rc != GDN_CUDA_OK)                                                                                    \
+			return _rc;                                                                                            \
+	} while (0)
+
+template <typename T, bool SP, bool METAL>
+static int prepare_rk3_one()
+{
+	typedef Rk3Variants<T> V;
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, V::lo, V::pf_lo, METAL>,
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, V::hi, V::pf_hi, METAL>,
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+	return GDN_CUDA_OK;
+}
+
 template <typename T>
 int prepare_rk3()
 {
-	typedef Rk3Variants<T> V;
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, V::lo, V::pf_lo>,
-									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, V::lo, V::pf_lo>,
-									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, true, V::hi, V::pf_hi>,
-									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, false, V::hi, V::pf_hi>,
-									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+	GDN_RK3_TRY((prepare_rk3_one<T, true, false>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, false, false>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, true, true>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, false, true>()));
 	return GDN_CUDA_OK;
+}
+
+template <typename T, bool SP, bool METAL>
+static void launch_rk3_one(const Rk3Params<T> &p, int variant, cudaStream_t s)
+{
+	typedef Rk3Variants<T> V;
+	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
+	const int sm = Rk3Smem<T>::bytes;
+	if (variant == 0)
+		rk3_stage_kernel<T, SP, V::lo, V::pf_lo, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
+	else
+		rk3_stage_kernel<T, SP, V::hi, V::pf_hi, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
 }
 
 // variant 0: register cap for Rk3MinBlocks::lo CTAs per SM, 1: for ::hi
 template <typename T>
 int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s)
 {
-	typedef Rk3Variants<T> V;
-	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
-	const int sm = Rk3Smem<T>::bytes;
-	if (variant == 0) {
-		if (p.sparse)
-			rk3_stage_kernel<T, true, V::lo, V::pf_lo><<<nblk, kRk3Threads, sm, s>>>(p);
+	if (p.sparse) {
+		if (p.bc_metal)
+			launch_rk3_one<T, true, true>(p, variant, s);
 		else
-			rk3_stage_kernel<T, false, V::lo, V::pf_lo><<<nblk, kRk3Threads, sm, s>>>(p);
+			launch_rk3_one<T, true, false>(p, variant, s);
 	} else {
-		if (p.sparse)
-			rk3_stage_kernel<T, true, V::hi, V::pf_hi><<<nblk, kRk3Threads, sm, s>>>(p);
+		if (p.bc_metal)
+			launch_rk3_one<T, false, true>(p, variant, s);
 		else
-			rk3_stage_kernel<T, false, V::hi, V::pf_hi><<<nblk, kRk3Threads, sm, s>>>(p);
+			launch_rk3_one<T, false, false>(p, variant, s);
 	}
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;

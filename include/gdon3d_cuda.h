@@ -92,6 +92,11 @@ typedef struct gdn_cuda_data {
  * velocity set. */
 #define GDN_CUDA_SCHEME_RK3 0
 #define GDN_CUDA_SCHEME_KINETIC 1
+/* model->get_num_flux_boundary of the RK3 scheme: maxwell_num_flux_upwind
+ * with the analytic data as the outside state, or
+ * maxwell_num_flux_boundary_metal (src/models/maxwell.c:205-223): (-n x H_L, 0). */
+#define GDN_CUDA_BC_UPWIND 0
+#define GDN_CUDA_BC_METAL 1
 typedef struct gdn_cuda_model {
 	int scheme;
 	int nb_w; /* must be 6 */
@@ -100,6 +105,8 @@ typedef struct gdn_cuda_model {
 	double omega; /* model->omega (relaxation) */
 	const double *vi; /* [3*nb_v] model->vi */
 	double theta; /* 0.5 in the reference (relaxation.c:133) */
+	int boundary_flux; /* GDN_CUDA_BC_*; the kinetic scheme uses f_eq of the
+	                      data (d3q4_get_fR) and takes GDN_CUDA_BC_UPWIND only */
 } gdn_cuda_model;
 
 #define GDN_CUDA_FP64 0 /* FP64 storage and arithmetic */

@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 SCHEME_RK3, SCHEME_D3Q4, SCHEME_D3Q6 = 0, 1, 2
+SCHEME_RK3_METAL = 3  # RK3 with the metal boundary flux (maxwell.c:205-223)
 DATA_PLANE, DATA_CAVITY = 0, 1
 
 

@@ -133,15 +133,18 @@ void ref_mesh_free(void *pm)
 	free(m);
 }
 
-/* scheme: 0 = RK3 Maxwell upwind, 1 = CFL-less d3q4, 2 = CFL-less d3q6 */
+/* scheme: 0 = RK3 Maxwell upwind, 1 = CFL-less d3q4, 2 = CFL-less d3q6,
+ * 3 = RK3 Maxwell upwind with the metal boundary flux
+ * (maxwell_num_flux_boundary_metal, src/models/maxwell.c:205-223) */
 static void setup_model(gdn_model *model, int scheme, const ref_data *d)
 {
 	memset(model, 0, sizeof(*model));
 	model->nb_w = 6;
 	model->get_num_flux = maxwell_num_flux_upwind;
-	model->get_num_flux_boundary = maxwell_num_flux_upwind;
+	model->get_num_flux_boundary =
+		scheme == 3 ? maxwell_num_flux_boundary_metal : maxwell_num_flux_upwind;
 	model->get_imposed_data = select_data(d);
-	if (scheme == 0) {
+	if (scheme == 0 || scheme == 3) {
 		model->use_relax_scheme = false;
 		model->lambda = 1.0;
 	} else {
@@ -158,7 +161,7 @@ static void setup_model(gdn_model *model, int scheme, const ref_data *d)
 int ref_wlen(void *pm, int scheme)
 {
 	gdn_mesh *m = (gdn_mesh *)pm;
-	int mm = scheme == 0 ? 6 : (scheme == 1 ? 24 : 36);
+	int mm = (scheme == 0 || scheme == 3) ? 6 : (scheme == 1 ? 24 : 36);
 	return mm * (10 * m->nbelems + 6 * m->nboundaryfaces);
 }
 

@@ -140,3 +140,27 @@ def test_graph_replay_equals_direct_launches(scheme):
         s.close()
         out.append((wn, t))
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("n,jitter", [(3, 0.0), (4, 0.15)])
+def test_rk3_metal_boundary_matches_reference(n, jitter):
+    """RK3 with the metal boundary flux (-n x H_L, 0) (maxwell.c:205-223) on
+    the PEC cavity mode, against the reference built with
+    maxwell_num_flux_boundary_metal as model->get_num_flux_boundary."""
+    c, e = kuhn.kuhn_cube(n, jitter, seed=4)
+    mesh = capi.mesh_build(c, e)
+    dt = 0.3 * mesh.hmin()
+    steps = 15
+    s = capi.Solver(mesh, capi.SCHEME_RK3, capi.cavity_data(), dt, boundary_flux=capi.BC_METAL)
+    wn, t, _ = s.solve(steps)
+    err = s.error_l2()
+    s.close()
+    r = ref.RefMesh(c, e).run(ref.SCHEME_RK3_METAL, ref.make_data(kind=ref.DATA_CAVITY), dt, steps)
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= FP64_RTOL, rel
+    assert abs(err - r["err"]) <= 1e-10 * r["err"]
+    # the metal flux differs from the upwind flux with the exact data
+    s2 = capi.Solver(mesh, capi.SCHEME_RK3, capi.cavity_data(), dt)
+    wu, _, _ = s2.solve(steps)
+    s2.close()
+    assert np.linalg.norm(wu - wn) > 1e-6 * np.linalg.norm(wn)
