@@ -78,7 +78,7 @@ EXPORTS = [
     "gdn_cuda_get_time", "gdn_cuda_state_size", "gdn_cuda_num_levels", "gdn_cuda_launch_count",
     "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc", "gdn_cuda_attach_batch",
     "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_variant",
-    "gdn_cuda_kin_sweep_mode",
+    "gdn_cuda_kin_sweep_mode", "gdn_cuda_time_convergence", "gdn_cuda_space_convergence",
 ]
 
 _lib = None
@@ -119,6 +119,11 @@ def lib():
     L.gdn_cuda_num_instances.argtypes = [vp, ip]
     L.gdn_cuda_rk3_variant.argtypes = [vp, ip, ip]
     L.gdn_cuda_kin_sweep_mode.argtypes = [vp, ip]
+    L.gdn_cuda_time_convergence.argtypes = [C.POINTER(Mesh), C.POINTER(Tables), C.POINTER(Model), C.POINTER(Data),
+                                            C.POINTER(Config), C.c_double, C.c_double, C.c_int, dp, ip, dp, dp]
+    L.gdn_cuda_space_convergence.argtypes = [C.POINTER(C.POINTER(Mesh)), C.c_int, C.POINTER(Tables),
+                                             C.POINTER(Model), C.POINTER(Data), C.POINTER(Config), C.c_double,
+                                             C.c_double, C.c_int, dp, ip, dp, dp, dp]
     L.gdn_cuda_instance_info.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                          C.POINTER(C.c_longlong)]
     _lib = L
@@ -408,3 +413,43 @@ class BatchSolver(Solver):
         e = np.zeros(self.ninst, np.float64)
         check(self.L.gdn_cuda_error_l2_batch(self.h, _dp(e)))
         return e
+
+
+def _conv_model(scheme, nb_v, boundary_flux):
+    holder = Solver.__new__(Solver)
+    model = Solver._model(holder, scheme, nb_v, 0.5, boundary_flux)
+    return holder, model
+
+
+def time_convergence(mesh: MeshArrays, scheme, data, init_dt: float, tmax: float, nb_run: int,
+                     precision=FP64, nb_v=4, boundary_flux=BC_UPWIND, tables: Tables = None, device=0):
+    """utils_l2_time_convergence on the device (gdn_cuda_time_convergence):
+    returns dict(dt, iter, err, order) arrays over the dt-halving runs."""
+    L = lib()
+    tabs = tables if tables is not None else t10_tables()
+    holder, model = _conv_model(scheme, nb_v, boundary_flux)
+    cfg = Config(precision, 1, 0, 1, device, 0)
+    dt, err, order = (np.zeros(nb_run) for _ in range(3))
+    it = np.zeros(nb_run, np.int32)
+    check(L.gdn_cuda_time_convergence(C.byref(mesh.struct), C.byref(tabs), C.byref(model), C.byref(data),
+                                      C.byref(cfg), float(init_dt), float(tmax), int(nb_run), _dp(dt), _ip(it),
+                                      _dp(err), _dp(order)))
+    return dict(dt=dt, iter=it, err=err, order=order)
+
+
+def space_convergence(meshes, scheme, data, init_dt: float, tmax: float, time_refinement=True, precision=FP64,
+                      nb_v=4, boundary_flux=BC_UPWIND, tables: Tables = None, device=0):
+    """utils_l2_space_convergence on the device (gdn_cuda_space_convergence):
+    returns dict(dt, iter, hmin, err, order) over the meshes."""
+    L = lib()
+    tabs = tables if tables is not None else t10_tables()
+    holder, model = _conv_model(scheme, nb_v, boundary_flux)
+    cfg = Config(precision, 1, 0, 1, device, 0)
+    n = len(meshes)
+    ptrs = (C.POINTER(Mesh) * n)(*[C.pointer(m.struct) for m in meshes])
+    dt, hmin, err, order = (np.zeros(n) for _ in range(4))
+    it = np.zeros(n, np.int32)
+    check(L.gdn_cuda_space_convergence(ptrs, n, C.byref(tabs), C.byref(model), C.byref(data), C.byref(cfg),
+                                       float(init_dt), float(tmax), int(bool(time_refinement)), _dp(dt), _ip(it),
+                                       _dp(hmin), _dp(err), _dp(order)))
+    return dict(dt=dt, iter=it, hmin=hmin, err=err, order=order)

@@ -1527,6 +1527,123 @@ extern "C" int gdn_cuda_error_l2_batch(gdn_cuda_handle *h, double *err)
 	return GDN_CUDA_OK;
 }
 
+// ------------------------------------------------------- convergence --
+// New time step of a single-instance RK3 handle: the step graphs hold the
+// old one in their kernel parameters and are captured again.
+static int rk3_set_dt(gdn_cuda_handle *h, double dt)
+{
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	h->hdt.assign(h->ninst, dt);
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->dt_dev, h->hdt.data(), h->ninst * sizeof(double), cudaMemcpyHostToDevice,
+								 h->stream));
+	for (int k = 0; k < 2; k++)
+		if (h->graph_exec[k]) {
+			cudaGraphExecDestroy(h->graph_exec[k]);
+			h->graph_exec[k] = nullptr;
+		}
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	return GDN_CUDA_OK;
+}
+
+// dg_solve + simulation_error_l2 of one run of a study
+static int conv_run(gdn_cuda_handle *h, int iter, double *err)
+{
+	GDN_TRY(gdn_cuda_init(h));
+	GDN_TRY(advance_impl(h, iter));
+	return error_l2_impl(h, 0, err);
+}
+
+// get_order (src/utils/convergence.c:25-41): log(e_prev / e) / log(x_prev / x)
+static double conv_order(double e_prev, double e, double x_prev, double x)
+{
+	return std::log(e_prev / e) / std::log(x_prev / x);
+}
+
+extern "C" int gdn_cuda_time_convergence(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
+										 const gdn_cuda_model *model, const gdn_cuda_data *data,
+										 const gdn_cuda_config *config, double init_dt, double tmax, int nb_run,
+										 double *dt_out, int *iter_out, double *err_out, double *order_out)
+{
+	if (nb_run < 1 || !dt_out || !iter_out || !err_out || !order_out || !model || !(init_dt > 0.0) ||
+		!std::isfinite(init_dt) || !std::isfinite(tmax))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "time_convergence: bad arguments");
+	// the reference's time grid: init_iter = floor(tmax / dt) - 1 steps, tmax
+	// rounded down to a multiple of dt, dt halved and the steps doubled per run
+	const int iter0 = (int)std::floor(tmax / init_dt) - 1;
+	if (iter0 < 1)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "time_convergence: tmax shorter than two steps");
+	const double tmax0 = iter0 * init_dt;
+	gdn_cuda_handle *h = nullptr;
+	int rc = GDN_CUDA_OK;
+	for (int k = 0; k < nb_run && rc == GDN_CUDA_OK; k++) {
+		const double dt = k == 0 ? init_dt : 0.5 * dt_out[k - 1];
+		const long long want = (long long)iter0 << k;
+		const long long iter = (long long)std::floor(tmax0 / dt);
+		if (iter != want || iter > 2147483647LL) {
+			rc = gdn_set_error(GDN_CUDA_ERR_INVALID, "time_convergence: the halved time grid does not reach tmax");
+			break;
+		}
+		if (h && model->scheme == GDN_CUDA_SCHEME_RK3) {
+			rc = rk3_set_dt(h, dt);
+		} else {
+			if (h)
+				gdn_cuda_detach(h);
+			h = nullptr;
+			rc = gdn_cuda_attach(mesh, tables, model, data, config, dt, &h);
+		}
+		if (rc == GDN_CUDA_OK)
+			rc = conv_run(h, (int)iter, &err_out[k]);
+		dt_out[k] = dt;
+		iter_out[k] = (int)iter;
+		order_out[k] = k == 0 ? -1.0 : conv_order(err_out[k - 1], err_out[k], dt_out[k - 1], dt);
+	}
+	if (h) {
+		std::string msg = g_last_error;
+		gdn_cuda_detach(h);
+		g_last_error = msg;
+	}
+	return rc;
+}
+
+extern "C" int gdn_cuda_space_convergence(const gdn_cuda_mesh *const *meshes, int nb_run,
+										  const gdn_cuda_tables *tables, const gdn_cuda_model *model,
+										  const gdn_cuda_data *data, const gdn_cuda_config *config, double init_dt,
+										  double tmax, int time_refinement, double *dt_out, int *iter_out,
+										  double *hmin_out, double *err_out, double *order_out)
+{
+	if (!meshes || nb_run < 1 || !dt_out || !iter_out || !hmin_out || !err_out || !order_out || !model ||
+		!(init_dt > 0.0) || !std::isfinite(init_dt) || !std::isfinite(tmax))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "space_convergence: bad arguments");
+	const int iter0 = (int)std::floor(tmax / init_dt) - 1;
+	if (iter0 < 1)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "space_convergence: tmax shorter than two steps");
+	const double tmax0 = iter0 * init_dt;
+	for (int k = 0; k < nb_run; k++) {
+		const double dt = k == 0 || !time_refinement ? init_dt : 0.5 * dt_out[k - 1];
+		const long long want = time_refinement ? (long long)iter0 << k : iter0;
+		const long long iter = (long long)std::floor(tmax0 / dt);
+		if (iter != want || iter > 2147483647LL)
+			return gdn_set_error(GDN_CUDA_ERR_INVALID, "space_convergence: the time grid does not reach tmax");
+		GDN_TRY(gdn_cuda_mesh_hmin(meshes[k], &hmin_out[k]));
+		// the reference asserts meshes refined by 2 (convergence.c:157)
+		if (k > 0 && !(std::fabs(hmin_out[k - 1] / hmin_out[k] - 2.0) < 1e-6))
+			return gdn_set_error(GDN_CUDA_ERR_INVALID, "space_convergence: consecutive meshes must halve hmin");
+		gdn_cuda_handle *h = nullptr;
+		GDN_TRY(gdn_cuda_attach(meshes[k], tables, model, data, config, dt, &h));
+		const int rc = conv_run(h, (int)iter, &err_out[k]);
+		std::string msg = g_last_error;
+		gdn_cuda_detach(h);
+		g_last_error = msg;
+		if (rc != GDN_CUDA_OK)
+			return rc;
+		dt_out[k] = dt;
+		iter_out[k] = (int)iter;
+		order_out[k] = k == 0 ? -1.0 : conv_order(err_out[k - 1], err_out[k], hmin_out[k - 1], hmin_out[k]);
+	}
+	return GDN_CUDA_OK;
+}
+
 extern "C" int gdn_cuda_get_time(gdn_cuda_handle *h, double *t)
 {
 	if (!h || !t)

@@ -238,6 +238,32 @@ int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, const double *
 							  const double *wpg, const gdn_cuda_data *data, double t, void *stream,
 							  double *err);
 
+/* ---- convergence studies ------------------------------------------------- */
+
+/* utils_l2_time_convergence (src/utils/convergence.c:43-104) on the device:
+ * nb_run solves of one problem from t = 0 to tmax' = init_iter * init_dt,
+ * init_iter = floor(tmax / init_dt) - 1, with dt halved (and the step count
+ * doubled) from one run to the next; an RK3 handle is reused across the runs,
+ * the kinetic scheme is attached again per run (its blocks depend on dt).
+ * Per run k: dt_out[k], iter_out[k], err_out[k] (simulation_error_l2 at
+ * tmax'), order_out[k] = log(err[k-1] / err[k]) / log 2 (-1 for k = 0). */
+int gdn_cuda_time_convergence(const gdn_cuda_mesh *mesh, const gdn_cuda_tables *tables,
+							  const gdn_cuda_model *model, const gdn_cuda_data *data,
+							  const gdn_cuda_config *config, double init_dt, double tmax,
+							  int nb_run, double *dt_out, int *iter_out, double *err_out,
+							  double *order_out);
+
+/* utils_l2_space_convergence (src/utils/convergence.c:106-168): one solve per
+ * mesh of meshes[nb_run] (each halving hmin_out of the previous one, checked
+ * like the reference), dt halved per run when time_refinement is non-zero;
+ * order_out[k] = log(err[k-1] / err[k]) / log(hmin[k-1] / hmin[k]). */
+int gdn_cuda_space_convergence(const gdn_cuda_mesh *const *meshes, int nb_run,
+							   const gdn_cuda_tables *tables, const gdn_cuda_model *model,
+							   const gdn_cuda_data *data, const gdn_cuda_config *config,
+							   double init_dt, double tmax, int time_refinement,
+							   double *dt_out, int *iter_out, double *hmin_out,
+							   double *err_out, double *order_out);
+
 /* ---- introspection ------------------------------------------------------ */
 int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
 int gdn_cuda_num_instances(gdn_cuda_handle *h, int *ninst);

@@ -162,3 +162,14 @@ def test_batch_attach_validates_instances():
     assert "one scheme" in L.gdn_cuda_last_error().decode()
     rc = L.gdn_cuda_attach_batch(inst, 0, C.byref(tabs), None, C.byref(h))
     assert rc == capi.ERR_INVALID
+
+
+def test_convergence_drivers_validate_before_touching_the_device():
+    c, e = kuhn.kuhn_cube(2)
+    m = capi.mesh_build(c, e)
+    with pytest.raises(capi.GdnError) as ex:
+        capi.time_convergence(m, capi.SCHEME_RK3, capi.plane_data(), 0.1, 0.15, 2)  # tmax < 2 steps
+    assert ex.value.code == capi.ERR_INVALID
+    with pytest.raises(capi.GdnError) as ex:
+        capi.time_convergence(m, capi.SCHEME_RK3, capi.plane_data(), 0.1, 1.0, 0)
+    assert ex.value.code == capi.ERR_INVALID
