@@ -361,71 +361,6 @@ static int build_neighbours(const gdn_cuda_mesh *m, const gdn_cuda_tables *t, st
 	return GDN_CUDA_OK;
 }
 
-// host Kahn scheduling of the upwind DAG per velocity; items grouped by
-// level (items[k] = e * nv + v, pos its inverse)
-static int build_schedule(gdn_cuda_handle *h, const std::vector<unsigned char> &mask,
-						  const std::vector<int> &nbv, std::vector<int> &items, std::vector<int> &pos,
-						  std::vector<int> &off)
-{
-	const long long ne = h->ne;
-	const int nv = h->nv;
-	std::vector<int> level(ne * nv, 0);
-	std::vector<int> indeg(ne);
-	std::vector<long long> queue(ne);
-	int maxlev = 0;
-	for (int v = 0; v < nv; v++) {
-		long long qh = 0, qt = 0;
-		for (long long e = 0; e < ne; e++) {
-			const unsigned char mk = mask[e * nv + v];
-			indeg[e] = __builtin_popcount(mk);
-			level[e * nv + v] = 0;
-			if (indeg[e] == 0)
-				queue[qt++] = e;
-		}
-		while (qh < qt) {
-			const long long e = queue[qh++];
-			const int le = level[e * nv + v];
-			for (int f = 0; f < 4; f++) {
-				const int d = nbv[4 * e + f];
-				if (d < 0)
-					continue;
-				// d depends on e iff d's mask has the face that points to e
-				const unsigned char md = mask[(long long)d * nv + v];
-				bool dep = false;
-				for (int g = 0; g < 4; g++)
-					if ((md >> g & 1) && nbv[4LL * d + g] == e)
-						dep = true;
-				if (!dep)
-					continue;
-				if (level[(long long)d * nv + v] < le + 1)
-					level[(long long)d * nv + v] = le + 1;
-				if (--indeg[d] == 0)
-					queue[qt++] = d;
-			}
-		}
-		if (qt != ne)
-			return gdn_set_error(GDN_CUDA_ERR_CYCLE, "attach: the upwind element graph has a cycle");
-		for (long long e = 0; e < ne; e++)
-			if (level[e * nv + v] > maxlev)
-				maxlev = level[e * nv + v];
-	}
-	const int nl = maxlev + 1;
-	off.assign(nl + 1, 0);
-	for (long long u = 0; u < ne * nv; u++)
-		off[level[u] + 1]++;
-	for (int l = 0; l < nl; l++)
-		off[l + 1] += off[l];
-	items.assign(ne * nv, 0);
-	pos.assign(ne * nv, 0);
-	std::vector<int> next(off.begin(), off.end() - 1);
-	for (long long u = 0; u < ne * nv; u++) {
-		const int k = next[level[u]]++;
-		items[k] = (int)u;
-		pos[u] = k;
-	}
-	return GDN_CUDA_OK;
-}
-
 template <typename S>
 static S *as(void *p)
 {
@@ -640,18 +575,14 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		// other kinetic array is stored in) is built on the host from them
 		GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->sown64, mask, s));
 		h->launches += 2;
-		std::vector<unsigned char> hmask(nu);
-		GDN_CUDA_TRY(cudaMemcpyAsync(hmask.data(), mask, nu, cudaMemcpyDeviceToHost, s));
-		GDN_CUDA_TRY(cudaStreamSynchronize(s));
-		std::vector<int> items, pos;
-		GDN_TRY(build_schedule(h, hmask, nb, items, pos, h->level_off));
 		GDN_TRY(dalloc(h, &h->items, nu));
 		GDN_TRY(dalloc(h, &h->pos, nu));
 		GDN_TRY(dalloc(h, &h->rnb, nu));
 		GDN_TRY(dalloc(h, &h->rpm, nu));
 		GDN_TRY(dalloc(h, &h->bt, 36LL * nv * (nbf > 0 ? nbf : 1)));
-		GDN_CUDA_TRY(cudaMemcpyAsync(h->items, items.data(), nu * sizeof(int), cudaMemcpyHostToDevice, s));
-		GDN_CUDA_TRY(cudaMemcpyAsync(h->pos, pos.data(), nu * sizeof(int), cudaMemcpyHostToDevice, s));
+		long long npasses = 0;
+		GDN_TRY(kin_device_schedule(mask, h->nb, ne, nv, h->items, h->pos, h->level_off, npasses, s));
+		h->launches += npasses + 3;
 		// state f: FP64 for FP64 and FP32_REFINE, FP32, or BF16
 		if (h->precision == GDN_CUDA_FP64 || h->precision == GDN_CUDA_FP32_REFINE)
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * nu));

@@ -1,6 +1,8 @@
 // Kernel parameter blocks and launchers shared between the translation units.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace gdn {
@@ -93,6 +95,13 @@ int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels
 					  int acc, int bdata, int sparse, cudaStream_t s);
 template <typename F, typename Y, typename T>
 int kin_levels_grid(int device, int acc, int sparse, int *grid);
+
+// Level schedule of the upwind item graph on the device: items[k] (e * nv +
+// v in level order, ascending within a level), pos (its inverse), level_off
+// (host, first item of each level, then the item count); GDN_CUDA_ERR_CYCLE
+// when the graph has a cycle.  npasses = relaxation passes used.
+int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, int nv, int *items, int *pos,
+						std::vector<int> &level_off, long long &npasses, cudaStream_t s);
 
 // f_eq of the analytic data at the boundary face nodes, t + dt/2 (FP64)
 int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Batch &b, int nv, const double *vi,

@@ -29,6 +29,10 @@
 #include <climits>
 #include <type_traits>
 
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
 #include <cuda_pipeline_primitives.h>
 
 #include "aux.h"
@@ -73,6 +77,135 @@ __global__ void kin_mask_kernel(const double *__restrict__ sown64, const int *__
 		if (nb[e * 4 + f] >= 0 && sown64[u * 4 + f] < 0.0)
 			m |= (unsigned char)(1 << f);
 	mask[u] = m;
+}
+
+// Level schedule on the device.  level(u) = the longest chain of upwind
+// dependencies ending at item u = e * nv + v (the levels Kahn's algorithm
+// yields), by in-place relaxation: each launch raises every level to one
+// more than its highest upwind dependency; levels only grow, and a pass
+// that changes nothing ends the iteration (at most depth + 1 passes).
+__global__ void kin_level_relax_kernel(const unsigned char *__restrict__ mask, const int *__restrict__ nb,
+									   long long ne, int nv, int *level, int *changed)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= ne * nv)
+		return;
+	const unsigned m = mask[u];
+	if (!m)
+		return;
+	const long long e = u / nv;
+	const int v = (int)(u % nv);
+	int l = 0;
+	for (int f = 0; f < 4; f++)
+		if (m >> f & 1) {
+			// other threads raise levels during the pass: read the current value
+			const int d = *(const volatile int *)(level + (long long)nb[e * 4 + f] * nv + v);
+			l = d + 1 > l ? d + 1 : l;
+		}
+	if (l > level[u]) {
+		level[u] = l;
+		*changed = 1;
+	}
+}
+
+__global__ void kin_iota_kernel(int *a, long long n)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u < n)
+		a[u] = (int)u;
+}
+
+// after the sort: pos = inverse of items, level_off[l] = first item of level l
+__global__ void kin_schedule_finish_kernel(const int *__restrict__ items, const int *__restrict__ lev_sorted,
+										   long long n, int *__restrict__ pos, int *__restrict__ level_off)
+{
+	const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (k >= n)
+		return;
+	pos[items[k]] = (int)k;
+	const int l = lev_sorted[k];
+	if (k == 0 || lev_sorted[k - 1] != l)
+		level_off[l] = (int)k;
+	if (k == n - 1)
+		level_off[l + 1] = (int)n;
+}
+
+int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, int nv, int *items, int *pos,
+						std::vector<int> &level_off, long long &npasses, cudaStream_t s)
+{
+	const long long nu = ne * nv;
+	const unsigned g = (unsigned)((nu + 255) / 256);
+	int *level = nullptr, *lev_sorted = nullptr, *iota = nullptr, *changed = nullptr, *loff = nullptr;
+	void *tmp = nullptr;
+	size_t tmp_bytes = 0;
+	int rc = GDN_CUDA_OK;
+	int h_changed = 1, maxlev = 0;
+	auto cleanup = [&]() {
+		cudaFree(level);
+		cudaFree(lev_sorted);
+		cudaFree(iota);
+		cudaFree(changed);
+		cudaFree(loff);
+		cudaFree(tmp);
+	};
+#define GDN_SCHED_TRY(expr)                                                                                           \
+	do {                                                                                                           \
+		cudaError_t _e = (expr);                                                                                   \
+		if (_e != cudaSuccess) {                                                                                   \
+			cleanup();                                                                                             \
+			return gdn_cuda_fail(_e, #expr, __FILE__, __LINE__);                                                  \
+		}                                                                                                          \
+	} while (0)
+	GDN_SCHED_TRY(cudaMalloc(&level, nu * sizeof(int)));
+	GDN_SCHED_TRY(cudaMalloc(&lev_sorted, nu * sizeof(int)));
+	GDN_SCHED_TRY(cudaMalloc(&iota, nu * sizeof(int)));
+	GDN_SCHED_TRY(cudaMalloc(&changed, sizeof(int)));
+	GDN_SCHED_TRY(cudaMemsetAsync(level, 0, nu * sizeof(int), s));
+	// a chain longer than the elements of one velocity repeats an element: a cycle
+	npasses = 0;
+	while (h_changed) {
+		if (npasses > ne + 1) {
+			cleanup();
+			return gdn_set_error(GDN_CUDA_ERR_CYCLE, "attach: the upwind element graph has a cycle");
+		}
+		GDN_SCHED_TRY(cudaMemsetAsync(changed, 0, sizeof(int), s));
+		kin_level_relax_kernel<<<g, 256, 0, s>>>(mask, nb, ne, nv, level, changed);
+		GDN_SCHED_TRY(cudaGetLastError());
+		GDN_SCHED_TRY(cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, s));
+		GDN_SCHED_TRY(cudaStreamSynchronize(s));
+		npasses++;
+	}
+	kin_iota_kernel<<<g, 256, 0, s>>>(iota, nu);
+	GDN_SCHED_TRY(cudaGetLastError());
+	// stable sort of the items by level: within a level the item order is
+	// ascending e * nv + v, as the host schedule had it
+	int bits = 1;
+	{
+		int *dmax = changed;
+		GDN_SCHED_TRY(cub::DeviceReduce::Max(nullptr, tmp_bytes, level, dmax, (int)nu, s));
+		GDN_SCHED_TRY(cudaMalloc(&tmp, tmp_bytes));
+		GDN_SCHED_TRY(cub::DeviceReduce::Max(tmp, tmp_bytes, level, dmax, (int)nu, s));
+		GDN_SCHED_TRY(cudaMemcpyAsync(&maxlev, dmax, sizeof(int), cudaMemcpyDeviceToHost, s));
+		GDN_SCHED_TRY(cudaStreamSynchronize(s));
+		cudaFree(tmp);
+		tmp = nullptr;
+		while ((1 << bits) <= maxlev)
+			bits++;
+	}
+	GDN_SCHED_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, level, lev_sorted, iota, items, (int)nu, 0,
+												  bits, s));
+	GDN_SCHED_TRY(cudaMalloc(&tmp, tmp_bytes));
+	GDN_SCHED_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, level, lev_sorted, iota, items, (int)nu, 0, bits,
+												  s));
+	GDN_SCHED_TRY(cudaMalloc(&loff, (maxlev + 2) * sizeof(int)));
+	kin_schedule_finish_kernel<<<g, 256, 0, s>>>(items, lev_sorted, nu, pos, loff);
+	GDN_SCHED_TRY(cudaGetLastError());
+	level_off.assign(maxlev + 2, 0);
+	GDN_SCHED_TRY(cudaMemcpyAsync(level_off.data(), loff, (maxlev + 2) * sizeof(int), cudaMemcpyDeviceToHost, s));
+	GDN_SCHED_TRY(cudaStreamSynchronize(s));
+#undef GDN_SCHED_TRY
+	cleanup();
+	return rc;
 }
 
 // G = D^-1 per (element, velocity), FP64 Gauss-Jordan with partial

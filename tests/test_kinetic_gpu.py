@@ -189,3 +189,15 @@ def test_kinetic_cooperative_sweep_equals_level_launches(precision, nb_v):
         s.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+
+
+@pytest.mark.parametrize("n,levels", [(16, 108), (64, 444)])
+def test_kinetic_device_schedule_levels(n, levels):
+    """The device-built level schedule has the depth of the upwind DAG that
+    Kahn's algorithm gives on the host for these Kuhn meshes (d3q4)."""
+    c, e = kuhn.kuhn_cube(n, 0.0, seed=1)
+    mesh = capi.mesh_build(c, e)
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), 3 * mesh.hmin(), precision=capi.FP32,
+                    kin_sweep=1)
+    assert s.num_levels == levels
+    s.close()
