@@ -333,7 +333,7 @@ def run_rk3(args, env):
     K = args.steps
     n = args.n or N_CUBE
     coords, e2n = kuhn.kuhn_cube(n, JITTER, seed=SEED)
-    mesh = capi.mesh_build(coords, e2n)
+    mesh = capi.mesh_build(coords, e2n, device=local)
     ne = mesh.nbelems
     dt = CFL * mesh.hmin()
     khat, kmag, pol = kuhn.random_plane_wave(SEED, KMAG)
@@ -480,7 +480,7 @@ def run_kinetic(args, env):
     K = args.steps
     n = args.n or KIN_N
     c, e = kuhn.kuhn_cube(n, 0.0, seed=SEED)
-    mesh = capi.mesh_build(c, e)
+    mesh = capi.mesh_build(c, e, device=env.local)
     ne = mesh.nbelems
     dt = KIN_MULT * CFL * mesh.hmin()
     data = capi.cavity_data()

@@ -79,6 +79,7 @@ EXPORTS = [
     "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc", "gdn_cuda_attach_batch",
     "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_variant",
     "gdn_cuda_kin_sweep_mode", "gdn_cuda_time_convergence", "gdn_cuda_space_convergence",
+    "gdn_cuda_mesh_build_gpu",
 ]
 
 _lib = None
@@ -96,6 +97,7 @@ def lib():
     L.gdn_cuda_t10_tables.argtypes = [C.POINTER(Tables)]
     L.gdn_cuda_mesh_build.argtypes = [C.c_int, dp, C.c_int, ip, ip, ip, ip, ip, ip, ip, ip, dp]
     L.gdn_cuda_mesh_hmin.argtypes = [C.POINTER(Mesh), dp]
+    L.gdn_cuda_mesh_build_gpu.argtypes = [C.c_int, dp, C.c_int, ip, ip, ip, ip, ip, ip, ip, ip, dp, C.c_int]
     L.gdn_cuda_attach.argtypes = [C.POINTER(Mesh), C.POINTER(Tables), C.POINTER(Model),
                                   C.POINTER(Data), C.POINTER(Config), C.c_double, C.POINTER(vp)]
     L.gdn_cuda_detach.argtypes = [vp]
@@ -201,23 +203,30 @@ class MeshArrays:
         return h.value
 
 
-def mesh_build(coords: np.ndarray, elem2node: np.ndarray) -> MeshArrays:
-    """mesh_build_connectivity-equivalent arrays from T4 vertices (0-based)."""
+def mesh_build(coords: np.ndarray, elem2node: np.ndarray, device=None) -> MeshArrays:
+    """mesh_build_connectivity-equivalent arrays from T4 vertices (0-based),
+    on the host (device=None) or on CUDA device `device` (same arrays)."""
     c = np.ascontiguousarray(coords, dtype=np.float64)
     e = np.ascontiguousarray(elem2node, dtype=np.int32)
     L = lib()
+    if device is None:
+        call = L.gdn_cuda_mesh_build
+        extra = ()
+    else:
+        call = L.gdn_cuda_mesh_build_gpu
+        extra = (int(device),)
     nf, nbf, nq = C.c_int(), C.c_int(), C.c_int()
     null_i = C.POINTER(C.c_int)()
     null_d = C.POINTER(C.c_double)()
-    check(L.gdn_cuda_mesh_build(len(c), _dp(c), len(e), _ip(e), C.byref(nf), C.byref(nbf),
-                                C.byref(nq), null_i, null_i, null_i, null_i, null_d))
+    check(call(len(c), _dp(c), len(e), _ip(e), C.byref(nf), C.byref(nbf), C.byref(nq), null_i, null_i, null_i,
+               null_i, null_d, *extra))
     f2e = np.zeros(4 * nf.value, np.int32)
     fn = np.zeros(12 * nf.value, np.int32)
     bf = np.zeros(max(nbf.value, 1), np.int32)
     e2q = np.zeros(10 * len(e) + 6 * nbf.value, np.int32)
     node = np.zeros(3 * nq.value, np.float64)
-    check(L.gdn_cuda_mesh_build(len(c), _dp(c), len(e), _ip(e), C.byref(nf), C.byref(nbf),
-                                C.byref(nq), _ip(f2e), _ip(fn), _ip(bf), _ip(e2q), _dp(node)))
+    check(call(len(c), _dp(c), len(e), _ip(e), C.byref(nf), C.byref(nbf), C.byref(nq), _ip(f2e), _ip(fn), _ip(bf),
+               _ip(e2q), _dp(node), *extra))
     return MeshArrays(f2e, fn, bf[:nbf.value], e2q, node, len(e))
 
 

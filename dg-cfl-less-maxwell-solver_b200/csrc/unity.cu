@@ -6,3 +6,4 @@
 #include "kinetic.cu"
 #include "api.cu"
 #include "noalloc.cu"
+#include "mesh_gpu.cu"

@@ -153,6 +153,15 @@ int gdn_cuda_mesh_build(int nbnodes, const double *coords, int nbelems,
 						int *fnode2enode, int *boundaryface, int *elem2qnode,
 						double *node);
 
+/* The same arrays as gdn_cuda_mesh_build, bit for bit, built on CUDA device
+ * `device` (face and edge matching by radix sorts, numbering by prefix sums);
+ * same size-query convention. */
+int gdn_cuda_mesh_build_gpu(int nbnodes, const double *coords, int nbelems,
+							const int *elem2node, int *nbfaces,
+							int *nboundaryfaces, int *nbqnodes, int *face2elem,
+							int *fnode2enode, int *boundaryface, int *elem2qnode,
+							double *node, int device);
+
 /* h_min = min over elements of volume / surface (mesh_get_t4_hmin,
  * src/mesh/mesh.c:149-210). */
 int gdn_cuda_mesh_hmin(const gdn_cuda_mesh *mesh, double *hmin);
