@@ -79,7 +79,7 @@ EXPORTS = [
     "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc", "gdn_cuda_attach_batch",
     "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_variant",
     "gdn_cuda_kin_sweep_mode", "gdn_cuda_time_convergence", "gdn_cuda_space_convergence",
-    "gdn_cuda_mesh_build_gpu",
+    "gdn_cuda_mesh_build_gpu", "gdn_cuda_save_xdmf",
 ]
 
 _lib = None
@@ -97,6 +97,7 @@ def lib():
     L.gdn_cuda_t10_tables.argtypes = [C.POINTER(Tables)]
     L.gdn_cuda_mesh_build.argtypes = [C.c_int, dp, C.c_int, ip, ip, ip, ip, ip, ip, ip, ip, dp]
     L.gdn_cuda_mesh_hmin.argtypes = [C.POINTER(Mesh), dp]
+    L.gdn_cuda_save_xdmf.argtypes = [vp, C.c_int, C.c_char_p, C.c_int]
     L.gdn_cuda_mesh_build_gpu.argtypes = [C.c_int, dp, C.c_int, ip, ip, ip, ip, ip, ip, ip, ip, dp, C.c_int]
     L.gdn_cuda_attach.argtypes = [C.POINTER(Mesh), C.POINTER(Tables), C.POINTER(Model),
                                   C.POINTER(Data), C.POINTER(Config), C.c_double, C.POINTER(vp)]
@@ -317,6 +318,10 @@ class Solver:
     def step_host(self, wn: np.ndarray, n: int):
         assert wn.dtype == np.float64 and wn.flags.c_contiguous
         check(self.L.gdn_cuda_step_host(self.h, _dp(wn), int(n)))
+
+    def save_xdmf(self, basename: str, iter_id: int, instance: int = 0):
+        """io_save_all of the current state (raw binary + XDMF files)."""
+        check(self.L.gdn_cuda_save_xdmf(self.h, int(instance), basename.encode(), int(iter_id)))
 
     def error_l2(self) -> float:
         e = C.c_double()

@@ -128,7 +128,7 @@ struct gdn_cuda_handle {
 	// Offsets of instance i: elements e_off[i], boundary faces bf_off[i],
 	// reference-layout state w_off[i] (m * neq_i values each).
 	int ninst = 1;
-	std::vector<long long> e_off, bf_off, w_off, neq_i;
+	std::vector<long long> e_off, bf_off, w_off, neq_i, q_off;
 	std::vector<Data> hdata;
 	std::vector<double> hdt, ht, ht_bdof; // host mirrors of dt, t, RK3 boundary-data time
 	int *einst = nullptr, *bfinst = nullptr; // nullptr for a single instance
@@ -721,6 +721,7 @@ static int concat_meshes(const gdn_cuda_instance *inst, int n, gdn_cuda_handle *
 	mc.node.resize(3 * nq);
 	long long e0 = 0, f0 = 0, b0 = 0, q0 = 0;
 	h->e_off.assign(1, 0);
+	h->q_off.assign(1, 0);
 	h->bf_off.assign(1, 0);
 	for (int i = 0; i < n; i++) {
 		const gdn_cuda_mesh *m = inst[i].mesh;
@@ -744,6 +745,7 @@ static int concat_meshes(const gdn_cuda_instance *inst, int n, gdn_cuda_handle *
 		f0 += m->nbfaces;
 		b0 += m->nboundaryfaces;
 		q0 += m->nbqnodes;
+		h->q_off.push_back(q0);
 		h->e_off.push_back(e0);
 		h->bf_off.push_back(b0);
 	}
@@ -837,6 +839,7 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 		mesh = &mc.m;
 	} else {
 		h->e_off = {0, mesh->nbelems};
+		h->q_off = {0, mesh->nbqnodes};
 		h->bf_off = {0, mesh->nboundaryfaces};
 	}
 	if (rc == GDN_CUDA_OK) {
@@ -1456,6 +1459,136 @@ extern "C" int gdn_cuda_error_l2_batch(gdn_cuda_handle *h, double *err)
 	for (int i = 0; i < h->ninst; i++)
 		GDN_TRY(error_l2_impl(h, i, err + i));
 	return GDN_CUDA_OK;
+}
+
+// ------------------------------------------------------------ output --
+// io_save_all (src/io/io_hdf5.c:355-368) with raw little-endian binary files
+// in place of HDF5 (libhdf5 is optional for this library): <base>_mesh_conn.bin
+// (int32 [ne][10] elem2qnode, instance-local), <base>_mesh_nodes.bin (float64
+// [nq][3]), <base>_data_%04d.bin (float64 [m][nq]: component im of node in
+// taken at its first element and first local node, io_hdf5.c:179-213), and
+// <base>_simulation_%04d.xmf describing them (Tet_10 topology; kinetic: the
+// distributions f%d and w%d = sum over velocities).
+static int write_file(const std::string &path, const void *data, size_t bytes)
+{
+	FILE *f = std::fopen(path.c_str(), "wb");
+	if (!f)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, ("save_xdmf: cannot open " + path).c_str());
+	const size_t w = bytes ? std::fwrite(data, 1, bytes, f) : 0;
+	const int closed = std::fclose(f);
+	if (w != bytes || closed != 0)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, ("save_xdmf: cannot write " + path).c_str());
+	return GDN_CUDA_OK;
+}
+
+static std::string base_name(const std::string &p)
+{
+	const size_t k = p.find_last_of('/');
+	return k == std::string::npos ? p : p.substr(k + 1);
+}
+
+extern "C" int gdn_cuda_save_xdmf(gdn_cuda_handle *h, int instance, const char *basename, int iter_id)
+{
+	if (!h || !basename || instance < 0 || instance >= h->ninst)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "save_xdmf: bad arguments");
+	GDN_TRY(check_device_error(h));
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	cudaStream_t s = h->stream;
+	const long long e0 = h->e_off[instance], ne = h->e_off[instance + 1] - e0;
+	const long long q0 = h->q_off[instance], nq = h->q_off[instance + 1] - q0;
+	const bool kin = h->scheme == GDN_CUDA_SCHEME_KINETIC;
+	const int m = kin ? 6 * h->nv : 6;
+	std::vector<int> conn(10 * ne);
+	std::vector<double> nodes(3 * nq), vals((size_t)m * nq);
+	int *owner = nullptr;
+	double *dv = nullptr;
+	cudaError_t ce = cudaMalloc(&owner, (nq > 0 ? nq : 1) * sizeof(int));
+	if (ce == cudaSuccess)
+		ce = cudaMalloc(&dv, ((size_t)m * nq > 0 ? (size_t)m * nq : 1) * sizeof(double));
+	int rc = ce == cudaSuccess ? GDN_CUDA_OK : gdn_cuda_fail(ce, "save_xdmf: cudaMalloc", __FILE__, __LINE__);
+	if (rc == GDN_CUDA_OK) {
+		const int sk = kin ? kin_state_kind(h) : (h->precision == GDN_CUDA_FP64 ? 0 : 1);
+		const void *st = kin ? h->f : h->w[h->cur];
+		rc = launch_node_values(st, sk, kin, h->nv, h->pos, h->e2q, e0, ne, q0, nq, owner, dv, s);
+		h->launches += 2;
+	}
+	if (rc == GDN_CUDA_OK) {
+		ce = cudaMemcpyAsync(vals.data(), dv, vals.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+		if (ce == cudaSuccess)
+			ce = cudaMemcpyAsync(conn.data(), h->e2q + 10 * e0, conn.size() * sizeof(int), cudaMemcpyDeviceToHost, s);
+		if (ce == cudaSuccess)
+			ce = cudaMemcpyAsync(nodes.data(), h->node + 3 * q0, nodes.size() * sizeof(double), cudaMemcpyDeviceToHost,
+								 s);
+		if (ce == cudaSuccess)
+			ce = cudaStreamSynchronize(s);
+		if (ce != cudaSuccess)
+			rc = gdn_cuda_fail(ce, "save_xdmf: read-back", __FILE__, __LINE__);
+	}
+	cudaFree(owner);
+	cudaFree(dv);
+	if (rc != GDN_CUDA_OK)
+		return rc;
+	for (auto &q : conn)
+		q -= (int)q0;
+	char buf[64];
+	const std::string base = basename;
+	std::snprintf(buf, sizeof(buf), "_data_%04d.bin", iter_id);
+	const std::string conn_f = base + "_mesh_conn.bin", node_f = base + "_mesh_nodes.bin", data_f = base + buf;
+	std::snprintf(buf, sizeof(buf), "_simulation_%04d.xmf", iter_id);
+	const std::string xmf_f = base + buf;
+	GDN_TRY(write_file(conn_f, conn.data(), conn.size() * sizeof(int)));
+	GDN_TRY(write_file(node_f, nodes.data(), nodes.size() * sizeof(double)));
+	GDN_TRY(write_file(data_f, vals.data(), vals.size() * sizeof(double)));
+	// data items refer to the binary files by name, next to the .xmf
+	const std::string cb = base_name(conn_f), nb = base_name(node_f), db = base_name(data_f);
+	std::string x;
+	char line[512];
+	x += "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n";
+	x += "<Xdmf Version=\"2.0\">\n<Domain>\n<Grid Name=\"TheMesh\">\n";
+	std::snprintf(line, sizeof(line), "<Time Value=\"%f\"/>\n", h->ht[instance]);
+	x += line;
+	std::snprintf(line, sizeof(line),
+				  "<Topology TopologyType=\"Tet_10\" NumberOfElements=\"%lld\">\n<DataItem Dimensions=\"%lld 10\" "
+				  "NumberType=\"Int\" Precision=\"4\" Format=\"Binary\" Endian=\"Little\">%s</DataItem>\n</Topology>\n",
+				  ne, ne, cb.c_str());
+	x += line;
+	std::snprintf(line, sizeof(line),
+				  "<Geometry GeometryType=\"XYZ\">\n<DataItem Dimensions=\"%lld 3\" NumberType=\"Float\" Precision=\"8\" "
+				  "Format=\"Binary\" Endian=\"Little\">%s</DataItem>\n</Geometry>\n",
+				  nq, nb.c_str());
+	x += line;
+	auto item = [&](int im, const char *indent) {
+		std::snprintf(line, sizeof(line),
+					  "%s<DataItem Dimensions=\"%lld 1\" NumberType=\"Float\" Precision=\"8\" Format=\"Binary\" "
+					  "Endian=\"Little\" Seek=\"%lld\">%s</DataItem>\n",
+					  indent, nq, (long long)im * nq * 8, db.c_str());
+		x += line;
+	};
+	const char *prefix = kin ? "f" : "w";
+	for (int im = 0; im < m; im++) {
+		std::snprintf(line, sizeof(line), "<Attribute Name=\"%s%d\" Center=\"Node\">\n", prefix, im);
+		x += line;
+		item(im, "");
+		x += "</Attribute>\n";
+	}
+	if (kin) { // macro variables w_iw = sum_iv f_(iw * nb_v + iv)
+		for (int iw = 0; iw < 6; iw++) {
+			std::snprintf(line, sizeof(line), "<Attribute Name=\"w%d\" Center=\"Node\">\n<DataItem ItemType=\"Function\" Function=\"",
+						  iw);
+			x += line;
+			for (int iv = 0; iv < h->nv; iv++) {
+				std::snprintf(line, sizeof(line), "%s$%d", iv ? "+" : "", iv);
+				x += line;
+			}
+			std::snprintf(line, sizeof(line), "\" Dimensions=\"%lld 1\">\n", nq);
+			x += line;
+			for (int iv = 0; iv < h->nv; iv++)
+				item(iw * h->nv + iv, "  ");
+			x += "</DataItem>\n</Attribute>\n";
+		}
+	}
+	x += "</Grid>\n</Domain>\n</Xdmf>\n";
+	return write_file(xmf_f, x.data(), x.size());
 }
 
 // ------------------------------------------------------- convergence --

@@ -389,4 +389,66 @@ template int launch_error_l2<__nv_bfloat16>(const __nv_bfloat16 *, int, long lon
 											const double *, const double *, long long, const Data &, double, double *,
 											int, double *, cudaStream_t);
 
+// Nodal values for output (io_hdf5.c:179-213): each P2 node of instance
+// elements [e0, e0 + ne) takes its dofs from the first element containing it
+// and the first local node there (node2elem is filled in element order,
+// mesh.c:1208-1221): the smallest 10 e + iloc.
+__global__ void io_owner_kernel(const int *__restrict__ e2q, long long e0, long long ne, long long q0, int *owner)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= ne * 10)
+		return;
+	atomicMin(owner + (e2q[10 * e0 + u] - q0), (int)u);
+}
+
+template <typename S>
+__global__ void io_values_kernel(const S *__restrict__ st, int kinetic, int nv, const int *__restrict__ pos,
+								 long long e0, long long nq, const int *__restrict__ owner, double *__restrict__ out)
+{
+	const long long in = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (in >= nq)
+		return;
+	const int u = owner[in];
+	if (u == 0x7f7f7f7f) { // a node no element uses (the fill value)
+		for (int im = 0; im < (kinetic ? 6 * nv : 6); im++)
+			out[im * nq + in] = 0.0;
+		return;
+	}
+	const long long e = e0 + u / 10;
+	const int i = u % 10;
+	if (!kinetic) {
+		for (int c = 0; c < 6; c++)
+			out[c * nq + in] = (double)Store<S>::load(st + rk3_tix(e, i * 6 + c));
+	} else {
+		// component im = iw * nv + iv of the reference's kinetic wn
+		for (int v = 0; v < nv; v++) {
+			const long long k = pos[e * nv + v];
+			for (int c = 0; c < 6; c++)
+				out[(c * nv + v) * nq + in] = (double)Store<S>::load(st + k * 60 + c * 10 + i);
+		}
+	}
+}
+
+int launch_node_values(const void *st, int sk, int kinetic, int nv, const int *pos, const int *e2q, long long e0,
+					   long long ne, long long q0, long long nq, int *owner, double *out, cudaStream_t s)
+{
+	if (nq <= 0)
+		return GDN_CUDA_OK;
+	GDN_CUDA_TRY(cudaMemsetAsync(owner, 0x7f, nq * sizeof(int), s)); // 0x7f7f7f7f: above every 10 e + i
+	io_owner_kernel<<<(unsigned)((ne * 10 + 255) / 256), 256, 0, s>>>(e2q, e0, ne, q0, owner);
+	GDN_CUDA_TRY(cudaGetLastError());
+	const unsigned g = (unsigned)((nq + 255) / 256);
+	if (sk == 0)
+		io_values_kernel<double><<<g, 256, 0, s>>>(reinterpret_cast<const double *>(st), kinetic, nv, pos, e0, nq,
+												   owner, out);
+	else if (sk == 1)
+		io_values_kernel<float><<<g, 256, 0, s>>>(reinterpret_cast<const float *>(st), kinetic, nv, pos, e0, nq,
+												  owner, out);
+	else
+		io_values_kernel<__nv_bfloat16><<<g, 256, 0, s>>>(reinterpret_cast<const __nv_bfloat16 *>(st), kinetic, nv,
+														   pos, e0, nq, owner, out);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+
 } // namespace gdn

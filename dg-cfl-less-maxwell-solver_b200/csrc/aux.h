@@ -32,4 +32,9 @@ int launch_error_l2(const S *state, int kinetic, long long e0, int nv, const int
 					const double *node, const double *geom, long long ne, const Data &d, double t, double *partial,
 					int nblk, double *out, cudaStream_t s);
 
+// nodal output values [m][nq] of instance elements [e0, e0 + ne) (sk: state
+// storage 0 FP64, 1 FP32, 2 BF16); owner = [nq] scratch
+int launch_node_values(const void *st, int sk, int kinetic, int nv, const int *pos, const int *e2q, long long e0,
+					   long long ne, long long q0, long long nq, int *owner, double *out, cudaStream_t s);
+
 } // namespace gdn

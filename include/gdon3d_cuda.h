@@ -86,7 +86,8 @@ typedef struct gdn_cuda_data {
 } gdn_cuda_data;
 
 /* The recognised gdn_model (src/models/model.h:41-62): Maxwell with the
- * upwind flux maxwell_num_flux_upwind (also as the boundary flux), either
+ * upwind flux maxwell_num_flux_upwind (as the boundary flux too, or
+ * maxwell_num_flux_boundary_metal for RK3: boundary_flux), either
  * through RK3 (use_relax_scheme = false) or through the CFL-less scheme with
  * the d3q4 (nb_v = 4, d3q4.c:17-42) or d3q6 (nb_v = 6, d3q6.c:18-47)
  * velocity set. */
@@ -246,6 +247,17 @@ int gdn_cuda_error_l2_batch(gdn_cuda_handle *h, double *err);
 int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, const double *det, long long nbelems,
 							  const double *wpg, const gdn_cuda_data *data, double t, void *stream,
 							  double *err);
+
+/* ---- output ----------------------------------------------------------------- */
+
+/* io_save_all (src/io/io_hdf5.c:355-368) of instance `instance` of the handle
+ * at its current state, with raw little-endian binary files instead of HDF5:
+ * <basename>_mesh_conn.bin (int32 [nbelems][10], elem2qnode), _mesh_nodes.bin
+ * (float64 [nbqnodes][3]), _data_<iter_id %04d>.bin (float64 [m][nbqnodes]:
+ * component im of node in taken at its first element and first local node,
+ * as io_hdf5_dump_data) and _simulation_<iter_id %04d>.xmf (XDMF 2, Tet_10;
+ * kinetic: attributes f<im> and w<iw> = sum over the velocities). */
+int gdn_cuda_save_xdmf(gdn_cuda_handle *h, int instance, const char *basename, int iter_id);
 
 /* ---- convergence studies ------------------------------------------------- */
 
