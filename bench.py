@@ -27,6 +27,8 @@ from __future__ import annotations
 
 import argparse
 import concurrent.futures
+import contextlib
+import ctypes
 import multiprocessing
 import importlib.util
 import json
@@ -160,6 +162,23 @@ def algorithmic_bytes_per_step(ne, b_s, b_g):
     return ne * (600 * b_s + 3 * (10 * b_g + 32))
 
 
+@contextlib.contextmanager
+def c_stdout_to_stderr():
+    """The reference's time loops print progress to the C stdout ("\\r[Info]
+    t = ..."); send file descriptor 1 to stderr meanwhile, so that stdout
+    carries only the JSON line."""
+    sys.stdout.flush()
+    libc = ctypes.CDLL(None)
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def cpu_reference_sample(steps=CPU_SAMPLE_STEPS, n=CPU_SAMPLE_N):
     """The reference's own RK3 (oracle/_ref) on this host's cores, all threads."""
     threads = os.cpu_count() or 1
@@ -171,7 +190,8 @@ def cpu_reference_sample(steps=CPU_SAMPLE_STEPS, n=CPU_SAMPLE_N):
     k, kmag, p = gk.random_plane_wave(SEED, KMAG)
     rm = ref.RefMesh(c, e)
     dt = CFL * rm.hmin()
-    r = rm.run(ref.SCHEME_RK3, ref.make_data(khat=k, kmag=kmag, pol=p), dt, steps)
+    with c_stdout_to_stderr():
+        r = rm.run(ref.SCHEME_RK3, ref.make_data(khat=k, kmag=kmag, pol=p), dt, steps)
     dofs = 10 * len(e) * 6 * 3 * steps
     return {"value": dofs / r["cpu_run"], "unit": "DoF-updates/s", "cores": threads,
             "kind": "reference",
@@ -191,7 +211,8 @@ def cpu_reference_kinetic_sample(steps=10, n=KIN_CPU_N):
     c, e = gk.kuhn_cube(n, 0.0, seed=SEED)
     rm = ref.RefMesh(c, e)
     dt = KIN_MULT * CFL * rm.hmin()
-    r = rm.run(ref.SCHEME_D3Q4, ref.make_data(kind=ref.DATA_CAVITY), dt, steps)
+    with c_stdout_to_stderr():
+        r = rm.run(ref.SCHEME_D3Q4, ref.make_data(kind=ref.DATA_CAVITY), dt, steps)
     dofs = 10 * len(e) * 24 * steps
     return {"value": dofs / r["cpu_run"], "unit": "DoF-updates/s", "cores": threads, "kind": "reference",
             "sample": "reference dg_solve_relaxation (oracle/_ref, -O3 -fopenmp, exact sparse LU shim) on a "

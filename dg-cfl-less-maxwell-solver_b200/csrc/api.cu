@@ -74,6 +74,7 @@ struct gdn_cuda_handle {
 	long long launches = 0;
 	int ssize = 8; // bytes per stored state value
 	int rk3_sparse = 1; // tables follow the P2 structural-zero pattern
+	int rk3_fact = 1; // and the derivative tables factor through the P1 basis
 	int bc_metal = 0; // RK3 boundary faces take the metal flux
 	// device arrays
 	std::vector<DevBuf> bufs;
@@ -218,6 +219,11 @@ static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
 			o.MinvP[m][j].x = o.Minv[2 * m][j];
 			o.MinvP[m][j].y = o.Minv[2 * m + 1][j];
 		}
+	double q4[4][10];
+	rk3_q4(t, q4);
+	for (int l = 0; l < 4; l++)
+		for (int j = 0; j < 10; j++)
+			o.Q4[l][j] = (T)q4[l][j];
 	o.n3scale = (T)(t->ref_normal[3][0] * std::sqrt(3.0));
 	for (int f = 0; f < 4; f++) {
 		for (int k = 0; k < 3; k++)
@@ -410,6 +416,7 @@ static int autotune_rk3(gdn_cuda_handle *h)
 	p.stage0 = 0;
 	p.write_k2 = 1;
 	p.sparse = h->rk3_sparse;
+	p.fact = h->rk3_fact;
 	p.bc_metal = h->bc_metal;
 	cudaEvent_t ev[2];
 	GDN_CUDA_TRY(cudaEventCreate(&ev[0]));
@@ -467,6 +474,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 	if (!rk3_tables_standard_faces(t))
 		return gdn_set_error(GDN_CUDA_ERR_UNSUPPORTED, "attach: face2node differs from the P2 convention");
 	h->rk3_sparse = rk3_tables_sparse(t) ? 1 : 0;
+	h->rk3_fact = h->rk3_sparse && rk3_tables_factor(t) ? 1 : 0;
 	GDN_TRY(upload_tables(t));
 	std::vector<int> nb, perm;
 	std::vector<double> bx;
@@ -807,7 +815,7 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 	h->use_graph = cfg.use_graph;
 	// RK3 stage kernel compiled for fewer (1) or more (2) resident CTAs per
 	// SM; 0 = timed at attach
-	h->rk3_variant = cfg.rk3_variant == 2 ? 1 : 0;
+	h->rk3_variant = cfg.rk3_variant > 0 ? cfg.rk3_variant - 1 : 0;
 	h->rk3_autotune = cfg.rk3_variant == 0;
 	h->kin_mode = cfg.kin_sweep == 2 ? 2 : 1;
 	h->kin_autotune = cfg.kin_sweep == 0;
@@ -917,6 +925,7 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 		p.stage0 = i == 0;
 		p.write_k2 = i < 2;
 		p.sparse = h->rk3_sparse;
+		p.fact = h->rk3_fact;
 		p.bc_metal = h->bc_metal;
 		if (h->nbf > 0) {
 			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, bt, RK_C[i], as<T>(h->btrace), h->stream));
@@ -1147,7 +1156,8 @@ static int check_device_error(gdn_cuda_handle *h)
 	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
 	if (e) {
 		GDN_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
-		GDN_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned), h->stream));
+		if (h->bar)
+			GDN_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned), h->stream));
 		GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
 		return gdn_set_error(GDN_CUDA_ERR_TIMEOUT, "kinetic sweep: a grid barrier wait timed out; the state is invalid");
 	}

@@ -36,6 +36,9 @@ struct Tables {
 	typename Vec2<T>::type D2p[NQN / 2][NQN];
 	typename Vec2<T>::type MinvP[NQN / 2][NQN];
 	T D[3][NQN][NQN];
+	// Q4[l][j] = 4 int lambda_l phi_j (lambda_l the P1 barycentric basis):
+	// D[k] = G_k (Q4 / 4) with G_k the P1 coefficients of d_k(phi_i)
+	T Q4[4][NQN];
 	T Minv[NQN][NQN];
 	T M[NQN][NQN];
 	T S[NQV][NQV];

@@ -36,10 +36,13 @@ struct Rk3Params {
 	int stage0; // k2 = -dt dw (no k2 read)
 	int write_k2; // 0 on the last stage: k2 is dead until the next stage 0
 	int sparse; // tables follow the P2 structural-zero pattern
+	int fact; // the derivative tables factor through the P1 basis (rk3_tables_factor)
 	int bc_metal; // boundary faces take the metal flux (-n x H_L, 0)
 };
 
 bool rk3_tables_sparse(const gdn_cuda_tables *t);
+bool rk3_tables_factor(const gdn_cuda_tables *t);
+void rk3_q4(const gdn_cuda_tables *t, double q4[4][10]);
 bool rk3_tables_standard_faces(const gdn_cuda_tables *t);
 
 // variant 0 / 1: the stage kernel compiled for fewer / more resident CTAs per
@@ -48,6 +51,7 @@ template <typename T>
 int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s);
 template <typename T>
 int prepare_rk3();
+
 int rk3_min_blocks(int precision_fp64, int variant);
 // reference layout [e][node][field] (FP64, elements 0..ne-1) <-> tiled layout
 // at elements e0 .. e0 + ne - 1

@@ -23,17 +23,20 @@
 // elements, value-major inside a tile (rk3_tix): value k of element e at
 // ((e / 32) * 60 + k) * 32 + e % 32.  A CTA owns one tile with 6 warps, lane =
 // element, so every per-element access of a warp is one coalesced 128-byte
-// (FP32) row and nothing is staged through shared memory:
+// (FP32) row:
+//   0  every thread starts the gathers of its 24 neighbour-trace values
+//      (face node jj = warp of the 4 faces), asynchronously into its own flux
+//      slots in shared memory (cp.async; FP64 with few CTAs per SM: into
+//      registers), so that phase 1 hides their latency;
 //   1  warp c (field c): the 10 nodal values of field c in registers (kept
-//      for the RK update), r_k = D_k w_c with the tables as constant-bank
-//      operands and the P2 structural zeros removed at compile time; only the
-//      two physical derivatives the curl needs go to shared memory;
+//      for the RK update) and the two physical weak derivatives the curl
+//      needs, through the P1 basis (p1_weak_derivative: d(phi_i) is linear)
+//      with the tables as constant-bank operands; they go to shared memory;
 //   2  warp jj: the upwind flux at face node jj of the 4 faces (own traces from
-//      the tile, neighbour traces gathered from global, issued at kernel
-//      start so that phase 1 hides their latency) to shared memory;
+//      the tile) to shared memory;
 //   -- the one barrier --
 //   3  warp c: R_c = curl part + sum_faces S F_c, lift by Minv, RK update with
-//      k2 (prefetched before the barrier), coalesced stores.
+//      k2 (loaded before the barrier), coalesced stores.
 #include <cmath>
 
 #include "common.cuh"
@@ -61,6 +64,32 @@ __host__ __device__ constexpr int f2n(int f, int j)
 {
 	constexpr int m[4][6] = {{0, 3, 2, 7, 9, 6}, {0, 1, 3, 4, 8, 7}, {0, 2, 1, 6, 5, 4}, {1, 2, 3, 5, 9, 8}};
 	return m[f][j];
+}
+
+// P2 edge nodes 4..9 and their end vertices (t10.c:37-42 face-node lists)
+__host__ __device__ constexpr int edge_end(int e, int side)
+{
+	constexpr int m[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+	return m[e][side];
+}
+
+// Physical weak derivative sum_k g_k . D_k w of a P2 field along one
+// direction through the P1 basis: d(phi_i) is linear, so
+// int d(phi_i) w_h = (vertex i) g_i (4 u_i - s), (edge p-q) 4 (g_p u_q + g_q u_p)
+// with u_l = int lambda_l w_h, s = sum_l u_l and g_l the derivative of
+// lambda_l along the direction.  v = 4 u; t = v - s (vertex terms).
+template <typename T>
+__device__ __forceinline__ void p1_weak_derivative(const T cd[3], const T v[4], const T t[4], T out[10])
+{
+	const T g[4] = {-(cd[0] + cd[1] + cd[2]), cd[0], cd[1], cd[2]};
+#pragma unroll
+	for (int i = 0; i < 4; i++)
+		out[i] = g[i] * t[i];
+#pragma unroll
+	for (int e = 0; e < 6; e++) {
+		const int a = edge_end(e, 0), b = edge_end(e, 1);
+		out[4 + e] = g[a] * v[b] + g[b] * v[a];
+	}
 }
 
 // r[k][i] = sum_j D_k[i][j] w[j] for the three reference directions, with the
@@ -118,6 +147,22 @@ __device__ __forceinline__ void lift_minv<float>(const Tables<float> &tb, const 
 
 constexpr int kRk3Threads = 192; // 6 warps, one 32-element tile
 
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+	return (unsigned)__cvta_generic_to_shared(p);
+}
+// one value global -> shared, asynchronous (no register holds it meanwhile)
+template <typename T>
+__device__ __forceinline__ void cp_async_value(T *dst, const T *src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(sizeof(T))
+				 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+	asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 template <typename T>
 struct Rk3Smem {
 	static constexpr int P = 33;
@@ -125,20 +170,19 @@ struct Rk3Smem {
 	static constexpr int bytes = (120 + 144) * P * (int)sizeof(T);
 };
 
-// The two autotuned variants: register cap (minimum resident CTAs per SM) and
-// whether the neighbour traces are prefetched at kernel start (24 live values
-// through the volume phase) or loaded in the flux phase.
+// The two autotuned CTA-per-tile variants: register cap (minimum resident
+// CTAs per SM) and how the neighbour traces are prefetched (rk3_tile).
 template <typename T>
 struct Rk3Variants;
 template <>
 struct Rk3Variants<float> {
 	static constexpr int lo = 4, hi = 5;
-	static constexpr bool pf_lo = true, pf_hi = true;
+	static constexpr int pf_lo = 2, pf_hi = 2; // PF_ASYNC: 80 / 64 registers, no spills
 };
 template <>
 struct Rk3Variants<double> {
 	static constexpr int lo = 2, hi = 3;
-	static constexpr bool pf_lo = true, pf_hi = false;
+	static constexpr int pf_lo = 1, pf_hi = 2; // PF_REG at 2 CTAs per SM, PF_ASYNC at 3
 };
 
 // Upwind flux with the halving folded into the face quantities: with
@@ -169,21 +213,24 @@ __device__ __forceinline__ void upwind_flux_h(const T wL[6], const T wR[6], cons
 	F[5] = (h[0] * sE[1] - h[1] * sE[0]) + r2 * (n[2] * nH - nn * dH[2]);
 }
 
-template <typename T, bool SPARSE, int MINB, bool PF, bool METAL>
-__global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<T> p)
+// One tile of 32 elements, phases 1-3 (all threads of the CTA call it: it
+// holds the barrier between phases 2 and 3).  Wt[k * 32] is value k of this
+// lane's element (global memory or a shared-memory copy of the tile), Gt[q *
+// 32] its geometry value q, Kin[k * 32] its k2 value k; nbp / pmp point at its
+// neighbour and face-node permutation rows.
+// Neighbour-trace prefetch: none (loaded in the flux phase), into registers
+// at the start, or copied asynchronously into shared memory at the start.
+enum { PF_NONE = 0, PF_REG = 1, PF_ASYNC = 2 };
+
+template <typename T, bool SPARSE, bool FACT, int PF, bool METAL>
+__device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, const T *Wt, const T *Gt,
+										 const T *Kin, const int4 *nbp, const int4 *pmp, T *sX, T *sF)
 {
 	constexpr int P = Rk3Smem<T>::P;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	T *sX = reinterpret_cast<T *>(smem_raw); // [120][P]
-	T *sF = sX + 120 * P; // [144][P]
-
 	const Tables<T> &tb = tab<T>();
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const long long tile = blockIdx.x;
 	const long long e = tile * 32 + lane;
 	const bool live = e < p.ne;
-	const T *Wt = p.w_in + tile * 60 * 32 + lane; // Wt[k * 32] = value k of element e
-	const T *Gt = p.geom + tile * 10 * 32 + lane;
 
 	int nbk[4] = {0, 0, 0, 0}, pmk[4] = {0, 0, 0, 0};
 	T cod[3][3], det = T(1);
@@ -204,24 +251,44 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 				out[c] = __ldg(g + c);
 		}
 	};
-	// with PF they are issued first so that the volume phase hides their latency
-	T wR[PF ? 4 : 1][6];
+	// Prefetched at the start so that the volume phase hides their latency:
+	// PF_REG into registers, PF_ASYNC into this thread's own flux slots of sF
+	// ((f * 6 + jj) * 6 + c, the slots its flux later overwrites).
+	T wR[PF == PF_REG ? 4 : 1][6];
 	if (live) {
-		const int4 nb4 = __ldg(reinterpret_cast<const int4 *>(p.nb) + e);
-		const int4 pm4 = __ldg(reinterpret_cast<const int4 *>(p.perm) + e);
+		const int4 nb4 = *nbp;
+		const int4 pm4 = *pmp;
 		nbk[0] = nb4.x, nbk[1] = nb4.y, nbk[2] = nb4.z, nbk[3] = nb4.w;
 		pmk[0] = pm4.x, pmk[1] = pm4.y, pmk[2] = pm4.z, pmk[3] = pm4.w;
-		if (PF) {
+		if (PF == PF_REG) {
 #pragma unroll
 			for (int f = 0; f < 4; f++)
-				load_wR(f, wR[PF ? f : 0]);
+				load_wR(f, wR[PF == PF_REG ? f : 0]);
+		}
+		if (PF == PF_ASYNC) {
+#pragma unroll
+			for (int f = 0; f < 4; f++) {
+				const int nbv = nbk[f];
+				const T *g;
+				int st;
+				if (nbv >= 0) {
+					g = p.w_in + rk3_tix(nbv, ((pmk[f] >> (4 * warp)) & 15) * 6);
+					st = 32;
+				} else {
+					g = p.btrace + ((long long)(-nbv - 1) * 6 + warp) * 6;
+					st = 1;
+				}
+#pragma unroll
+				for (int cc = 0; cc < 6; cc++)
+					cp_async_value<T>(sF + ((f * 6 + warp) * 6 + cc) * P + lane, g + cc * st);
+			}
 		}
 #pragma unroll
 		for (int r = 0; r < 3; r++)
 #pragma unroll
 			for (int q = 0; q < 3; q++)
-				cod[r][q] = __ldg(Gt + (3 * r + q) * 32);
-		det = __ldg(Gt + 9 * 32);
+				cod[r][q] = Gt[(3 * r + q) * 32];
+		det = Gt[9 * 32];
 	}
 
 	// ---- 1: reference derivatives of field c = warp, two physical directions ----
@@ -239,12 +306,38 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 			cd1[k] = d1 == 0 ? cod[0][k] : (d1 == 1 ? cod[1][k] : cod[2][k]);
 			cd2[k] = d2 == 0 ? cod[0][k] : (d2 == 1 ? cod[1][k] : cod[2][k]);
 		}
-		T r[3][10];
-		ref_derivatives<T, SPARSE>(tb, w, r);
+		if (FACT) {
+			// v = Q4 w (the vertex diagonal of Q4 is zero), then the two
+			// directions through the P1 basis: 79 FMA instead of 273
+			T v[4], t[4], o1[10], o2[10];
 #pragma unroll
-		for (int i = 0; i < 10; i++) {
-			sX[((c * 2 + 0) * 10 + i) * P + lane] = cd1[0] * r[0][i] + cd1[1] * r[1][i] + cd1[2] * r[2][i];
-			sX[((c * 2 + 1) * 10 + i) * P + lane] = cd2[0] * r[0][i] + cd2[1] * r[1][i] + cd2[2] * r[2][i];
+			for (int l = 0; l < 4; l++) {
+				T acc = T(0);
+#pragma unroll
+				for (int j = 0; j < 10; j++)
+					if (j != l)
+						acc += tb.Q4[l][j] * w[j];
+				v[l] = acc;
+			}
+			const T s = T(0.25) * ((v[0] + v[1]) + (v[2] + v[3]));
+#pragma unroll
+			for (int l = 0; l < 4; l++)
+				t[l] = v[l] - s;
+			p1_weak_derivative<T>(cd1, v, t, o1);
+			p1_weak_derivative<T>(cd2, v, t, o2);
+#pragma unroll
+			for (int i = 0; i < 10; i++) {
+				sX[((c * 2 + 0) * 10 + i) * P + lane] = o1[i];
+				sX[((c * 2 + 1) * 10 + i) * P + lane] = o2[i];
+			}
+		} else {
+			T r[3][10];
+			ref_derivatives<T, SPARSE>(tb, w, r);
+#pragma unroll
+			for (int i = 0; i < 10; i++) {
+				sX[((c * 2 + 0) * 10 + i) * P + lane] = cd1[0] * r[0][i] + cd1[1] * r[1][i] + cd1[2] * r[2][i];
+				sX[((c * 2 + 1) * 10 + i) * P + lane] = cd2[0] * r[0][i] + cd2[1] * r[1][i] + cd2[2] * r[2][i];
+			}
 		}
 	}
 
@@ -264,8 +357,15 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 #pragma unroll
 			for (int a2 = 0; a2 < 3; a2++)
 				vn[a2] = f < 3 ? -cod[a2][f] : (cod[a2][0] + cod[a2][1] + cod[a2][2]) * tb.n3scale;
-			if (!PF)
+			if (PF == PF_ASYNC) {
+				if (f == 0)
+					cp_async_wait_all();
+#pragma unroll
+				for (int cc = 0; cc < 6; cc++)
+					wR[0][cc] = sF[((f * 6 + jj) * 6 + cc) * P + lane];
+			} else if (PF == PF_NONE) {
 				load_wR(f, wR[0]);
+			}
 			if (METAL && nbk[f] < 0) {
 				// maxwell_num_flux_boundary_metal (maxwell.c:205-223)
 				F[0] = vn[2] * wL[4] - vn[1] * wL[5];
@@ -273,7 +373,7 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 				F[2] = -vn[0] * wL[4] + vn[1] * wL[3];
 				F[3] = F[4] = F[5] = T(0);
 			} else {
-				upwind_flux_h<T>(wL, wR[PF ? f : 0], vn, F);
+				upwind_flux_h<T>(wL, wR[PF == PF_REG ? f : 0], vn, F);
 			}
 #pragma unroll
 			for (int cc = 0; cc < 6; cc++)
@@ -285,7 +385,7 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 	if (live && !p.stage0) {
 #pragma unroll
 		for (int i = 0; i < 10; i++)
-			k2o[i] = Kt[(i * 6 + c) * 32];
+			k2o[i] = Kin[(i * 6 + c) * 32];
 	}
 
 	__syncthreads();
@@ -333,6 +433,23 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 	}
 }
 
+// One CTA per tile, everything read from global memory.
+template <typename T, bool SPARSE, bool FACT, int MINB, int PF, bool METAL>
+__global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<T> p)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T *sX = reinterpret_cast<T *>(smem_raw); // [120][P]
+	T *sF = sX + 120 * Rk3Smem<T>::P; // [144][P]
+	const long long tile = blockIdx.x;
+	const int lane = threadIdx.x & 31;
+	const long long e = tile * 32 + lane;
+	const long long ec = e < p.ne ? e : p.ne - 1;
+	const T *Wt = p.w_in + tile * 60 * 32 + lane;
+	rk3_tile<T, SPARSE, FACT, PF, METAL>(p, tile, Wt, p.geom + tile * 10 * 32 + lane, p.k2 + tile * 60 * 32 + lane,
+										 reinterpret_cast<const int4 *>(p.nb) + ec,
+										 reinterpret_cast<const int4 *>(p.perm) + ec, sX, sF);
+}
+
 // P2 structural-zero pattern check for the tables handed to attach.
 bool rk3_tables_sparse(const gdn_cuda_tables *t)
 {
@@ -345,6 +462,53 @@ bool rk3_tables_sparse(const gdn_cuda_tables *t)
 		for (int j = 0; j < 6; j++)
 			if (!(smask(i) >> j & 1) && t->face_scal[i][j] != 0.0)
 				return false;
+	return true;
+}
+
+// Q4[l][j] = 4 int lambda_l phi_j = 4 sum_m lambda_l(x_m) M[m][j] (lambda_l is
+// linear, so its P2 interpolant is exact); the vertex diagonal is zero for
+// the P2 basis and is set to zero (rk3_tables_factor checks the whole
+// product).
+void rk3_q4(const gdn_cuda_tables *t, double q4[4][10])
+{
+	for (int l = 0; l < 4; l++)
+		for (int j = 0; j < 10; j++) {
+			double acc = t->mass[l][j];
+			for (int e = 0; e < 6; e++)
+				if (edge_end(e, 0) == l || edge_end(e, 1) == l)
+					acc += 0.5 * t->mass[4 + e][j];
+			q4[l][j] = j == l ? 0.0 : 4.0 * acc;
+		}
+}
+
+// D_k[i][j] = sum_l G_k[i][l] Q4[l][j] / 4 with G_k the P1 coefficients of
+// d_k(phi_i) (reference vertices 0, e_0, e_1, e_2), to 1e-15.
+bool rk3_tables_factor(const gdn_cuda_tables *t)
+{
+	double q4[4][10];
+	rk3_q4(t, q4);
+	for (int k = 0; k < 3; k++) {
+		double dl[4] = {-1.0, 0.0, 0.0, 0.0}; // d_k lambda_l
+		dl[k + 1] = 1.0;
+		for (int i = 0; i < 10; i++) {
+			double G[4] = {0.0, 0.0, 0.0, 0.0};
+			if (i < 4) {
+				for (int l = 0; l < 4; l++)
+					G[l] = dl[i] * (l == i ? 3.0 : -1.0);
+			} else {
+				const int a = edge_end(i - 4, 0), b = edge_end(i - 4, 1);
+				G[a] += 4.0 * dl[b];
+				G[b] += 4.0 * dl[a];
+			}
+			for (int j = 0; j < 10; j++) {
+				double d = 0.0;
+				for (int l = 0; l < 4; l++)
+					d += G[l] * 0.25 * q4[l][j];
+				if (!(std::fabs(d - t->internal[i][j][k]) <= 1e-15))
+					return false;
+			}
+		}
+	}
 	return true;
 }
 
@@ -372,13 +536,13 @@ bool rk3_tables_standard_faces(const gdn_cuda_tables *t)
 			return _rc;                                                                                            \
 	} while (0)
 
-template <typename T, bool SP, bool METAL>
+template <typename T, bool SP, bool FA, bool METAL>
 static int prepare_rk3_one()
 {
 	typedef Rk3Variants<T> V;
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, V::lo, V::pf_lo, METAL>,
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, FA, V::lo, V::pf_lo, METAL>,
 									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
-	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, V::hi, V::pf_hi, METAL>,
+	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, FA, V::hi, V::pf_hi, METAL>,
 									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
 	return GDN_CUDA_OK;
 }
@@ -386,40 +550,46 @@ static int prepare_rk3_one()
 template <typename T>
 int prepare_rk3()
 {
-	GDN_RK3_TRY((prepare_rk3_one<T, true, false>()));
-	GDN_RK3_TRY((prepare_rk3_one<T, false, false>()));
-	GDN_RK3_TRY((prepare_rk3_one<T, true, true>()));
-	GDN_RK3_TRY((prepare_rk3_one<T, false, true>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, true, true, false>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, true, false, false>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, false, false, false>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, true, true, true>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, true, false, true>()));
+	GDN_RK3_TRY((prepare_rk3_one<T, false, false, true>()));
 	return GDN_CUDA_OK;
 }
 
-template <typename T, bool SP, bool METAL>
+template <typename T, bool SP, bool FA, bool METAL>
 static void launch_rk3_one(const Rk3Params<T> &p, int variant, cudaStream_t s)
 {
 	typedef Rk3Variants<T> V;
 	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
 	const int sm = Rk3Smem<T>::bytes;
 	if (variant == 0)
-		rk3_stage_kernel<T, SP, V::lo, V::pf_lo, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
+		rk3_stage_kernel<T, SP, FA, V::lo, V::pf_lo, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
 	else
-		rk3_stage_kernel<T, SP, V::hi, V::pf_hi, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
+		rk3_stage_kernel<T, SP, FA, V::hi, V::pf_hi, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
 }
 
-// variant 0: register cap for Rk3MinBlocks::lo CTAs per SM, 1: for ::hi
+template <typename T, bool METAL>
+static void launch_rk3_tables(const Rk3Params<T> &p, int variant, cudaStream_t s)
+{
+	if (p.sparse && p.fact)
+		launch_rk3_one<T, true, true, METAL>(p, variant, s);
+	else if (p.sparse)
+		launch_rk3_one<T, true, false, METAL>(p, variant, s);
+	else
+		launch_rk3_one<T, false, false, METAL>(p, variant, s);
+}
+
+// variant 0: register cap for Rk3Variants::lo CTAs per SM, 1: for ::hi
 template <typename T>
 int launch_rk3_stage(const Rk3Params<T> &p, int variant, cudaStream_t s)
 {
-	if (p.sparse) {
-		if (p.bc_metal)
-			launch_rk3_one<T, true, true>(p, variant, s);
-		else
-			launch_rk3_one<T, true, false>(p, variant, s);
-	} else {
-		if (p.bc_metal)
-			launch_rk3_one<T, false, true>(p, variant, s);
-		else
-			launch_rk3_one<T, false, false>(p, variant, s);
-	}
+	if (p.bc_metal)
+		launch_rk3_tables<T, true>(p, variant, s);
+	else
+		launch_rk3_tables<T, false>(p, variant, s);
 	GDN_CUDA_TRY(cudaGetLastError());
 	return GDN_CUDA_OK;
 }

@@ -164,3 +164,47 @@ def test_rk3_metal_boundary_matches_reference(n, jitter):
     wu, _, _ = s2.solve(steps)
     s2.close()
     assert np.linalg.norm(wu - wn) > 1e-6 * np.linalg.norm(wn)
+
+
+_REF15 = {}
+
+
+def _ref15(kind):
+    """The reference build on a 15^3 x 6 mesh (20250 tets: a partial last
+    tile, and more tiles than a persistent grid holds), 20 steps."""
+    if kind not in _REF15:
+        c, e = kuhn.kuhn_cube(15, 0.1, seed=8)
+        mesh = capi.mesh_build(c, e)
+        dt = 0.3 * mesh.hmin()
+        if kind == "plane":
+            r = ref.RefMesh(c, e).run(ref.SCHEME_RK3, ref.make_data(khat=(0.6, 0.8, 0.0), kmag=4 * np.pi,
+                                                                   pol=(0, 0, 1)), dt, 20)
+        else:
+            r = ref.RefMesh(c, e).run(ref.SCHEME_RK3_METAL, ref.make_data(kind=ref.DATA_CAVITY), dt, 20)
+        _REF15[kind] = (mesh, dt, r)
+    return _REF15[kind]
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.FP32])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_rk3_every_stage_variant_matches_reference(variant, precision):
+    """Each stage kernel variant (two register budgets and neighbour-trace
+    prefetch modes) against the reference build."""
+    mesh, dt, r = _ref15("plane")
+    s = capi.Solver(mesh, capi.SCHEME_RK3, capi.plane_data(khat=(0.6, 0.8, 0.0), kmag=4 * np.pi, pol=(0, 0, 1)),
+                    dt, precision=precision, rk3_variant=variant)
+    assert s.rk3_variant[0] == variant
+    wn, t, _ = s.solve(20)
+    s.close()
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= (FP64_RTOL if precision == capi.FP64 else 2e-5), rel
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_rk3_variants_metal_boundary(variant):
+    mesh, dt, r = _ref15("metal")
+    s = capi.Solver(mesh, capi.SCHEME_RK3, capi.cavity_data(), dt, rk3_variant=variant, boundary_flux=capi.BC_METAL)
+    wn, _, _ = s.solve(20)
+    s.close()
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= FP64_RTOL, rel
