@@ -75,6 +75,7 @@ struct gdn_cuda_handle {
 	int ssize = 8; // bytes per stored state value
 	int rk3_sparse = 1; // tables follow the P2 structural-zero pattern
 	int rk3_fact = 1; // and the derivative tables factor through the P1 basis
+	int num_sms = 148; // SMs of the device
 	int bc_metal = 0; // RK3 boundary faces take the metal flux
 	// device arrays
 	std::vector<DevBuf> bufs;
@@ -417,6 +418,8 @@ static int autotune_rk3(gdn_cuda_handle *h)
 	p.write_k2 = 1;
 	p.sparse = h->rk3_sparse;
 	p.fact = h->rk3_fact;
+	p.num_sms = h->num_sms;
+	p.l2_ahead = 1;
 	p.bc_metal = h->bc_metal;
 	cudaEvent_t ev[2];
 	GDN_CUDA_TRY(cudaEventCreate(&ev[0]));
@@ -463,6 +466,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 {
 	const long long ne = h->ne, nf = h->nf, nbf = h->nbf;
 	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	GDN_CUDA_TRY(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
 	// The kinetic step is a chain of small dependent sweep launches whose
 	// time is latency: its stream gets the highest priority, so that its CTAs
 	// are dispatched ahead of pending CTAs of throughput work (an RK3 batch)
@@ -926,6 +930,8 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 		p.write_k2 = i < 2;
 		p.sparse = h->rk3_sparse;
 		p.fact = h->rk3_fact;
+		p.num_sms = h->num_sms;
+		p.l2_ahead = 1;
 		p.bc_metal = h->bc_metal;
 		if (h->nbf > 0) {
 			GDN_TRY(launch_boundary_trace<T>(h->bxyz, h->nbf, bt, RK_C[i], as<T>(h->btrace), h->stream));

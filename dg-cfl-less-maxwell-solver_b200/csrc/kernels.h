@@ -38,6 +38,8 @@ struct Rk3Params {
 	int sparse; // tables follow the P2 structural-zero pattern
 	int fact; // the derivative tables factor through the P1 basis (rk3_tables_factor)
 	int bc_metal; // boundary faces take the metal flux (-n x H_L, 0)
+	int num_sms; // SMs of the device
+	int l2_ahead; // nonzero: prefetch into L2 the tile this many CTAs ahead (set per variant at launch)
 };
 
 bool rk3_tables_sparse(const gdn_cuda_tables *t);

@@ -162,12 +162,19 @@ __device__ __forceinline__ void cp_async_wait_all()
 {
 	asm volatile("cp.async.wait_all;" ::: "memory");
 }
+// bring [p, p + bytes) into L2 (16-byte aligned, a multiple of 16 bytes)
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
+{
+	asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 
 template <typename T>
 struct Rk3Smem {
 	static constexpr int P = 33;
-	// sX: (field*2 + which)*10 + node, 120 rows; sF: (face*6 + jj)*6 + c, 144 rows
+	// sX: (field*2 + which)*10 + node, 120 rows (table-product path only);
+	// sF: (face*6 + jj)*6 + c, 144 rows
 	static constexpr int bytes = (120 + 144) * P * (int)sizeof(T);
+	static constexpr int bytes_fact = 144 * P * (int)sizeof(T);
 };
 
 // The two autotuned CTA-per-tile variants: register cap (minimum resident
@@ -177,7 +184,7 @@ struct Rk3Variants;
 template <>
 struct Rk3Variants<float> {
 	static constexpr int lo = 4, hi = 5;
-	static constexpr int pf_lo = 2, pf_hi = 2; // PF_ASYNC: 80 / 64 registers, no spills
+	static constexpr int pf_lo = 2, pf_hi = 2; // PF_ASYNC: 77 / 64 registers
 };
 template <>
 struct Rk3Variants<double> {
@@ -291,7 +298,9 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 		det = Gt[9 * 32];
 	}
 
-	// ---- 1: reference derivatives of field c = warp, two physical directions ----
+	// ---- 1: field c = warp in registers (kept for the RK update); the
+	// table-product path also computes its two physical derivatives for the
+	// curl into sX (FACT computes the curl's derivatives in phase 3) ----
 	const int c = warp;
 	const int a = c % 3;
 	T w[10];
@@ -299,6 +308,8 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 #pragma unroll
 		for (int j = 0; j < 10; j++)
 			w[j] = Wt[(j * 6 + c) * 32];
+	}
+	if (!FACT && live) {
 		const int d1 = (a + 1) % 3, d2 = (a + 2) % 3;
 		T cd1[3], cd2[3];
 #pragma unroll
@@ -306,31 +317,7 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 			cd1[k] = d1 == 0 ? cod[0][k] : (d1 == 1 ? cod[1][k] : cod[2][k]);
 			cd2[k] = d2 == 0 ? cod[0][k] : (d2 == 1 ? cod[1][k] : cod[2][k]);
 		}
-		if (FACT) {
-			// v = Q4 w (the vertex diagonal of Q4 is zero), then the two
-			// directions through the P1 basis: 79 FMA instead of 273
-			T v[4], t[4], o1[10], o2[10];
-#pragma unroll
-			for (int l = 0; l < 4; l++) {
-				T acc = T(0);
-#pragma unroll
-				for (int j = 0; j < 10; j++)
-					if (j != l)
-						acc += tb.Q4[l][j] * w[j];
-				v[l] = acc;
-			}
-			const T s = T(0.25) * ((v[0] + v[1]) + (v[2] + v[3]));
-#pragma unroll
-			for (int l = 0; l < 4; l++)
-				t[l] = v[l] - s;
-			p1_weak_derivative<T>(cd1, v, t, o1);
-			p1_weak_derivative<T>(cd2, v, t, o2);
-#pragma unroll
-			for (int i = 0; i < 10; i++) {
-				sX[((c * 2 + 0) * 10 + i) * P + lane] = o1[i];
-				sX[((c * 2 + 1) * 10 + i) * P + lane] = o2[i];
-			}
-		} else {
+		{
 			T r[3][10];
 			ref_derivatives<T, SPARSE>(tb, w, r);
 #pragma unroll
@@ -397,11 +384,46 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 	const int X = c / 3, b = a;
 	const int fa = 3 * (1 - X) + (b + 2) % 3; // field whose "d2" slot holds d_{b+1}
 	const int fb = 3 * (1 - X) + (b + 1) % 3; // field whose "d1" slot holds d_{b+2}
-	const T sgn = X == 0 ? T(1) : T(-1);
 	T R[10];
+	if (FACT) {
+		// d_{b+1} of field fa and d_{b+2} of field fb through the P1 basis
+		// (p1_weak_derivative), their rows read back from the tile (L1)
+		T o[2][10];
 #pragma unroll
-	for (int i = 0; i < 10; i++)
-		R[i] = sgn * (sX[((fa * 2 + 1) * 10 + i) * P + lane] - sX[((fb * 2 + 0) * 10 + i) * P + lane]);
+		for (int h = 0; h < 2; h++) {
+			const int fld = h ? fb : fa;
+			const int d = (b + 1 + h) % 3;
+			T wf[10], v[4], t[4], cd[3];
+#pragma unroll
+			for (int j = 0; j < 10; j++)
+				wf[j] = Wt[(j * 6 + fld) * 32];
+#pragma unroll
+			for (int l = 0; l < 4; l++) {
+				T acc = T(0);
+#pragma unroll
+				for (int j = 0; j < 10; j++)
+					if (j != l)
+						acc += tb.Q4[l][j] * wf[j];
+				v[l] = acc;
+			}
+			const T s = T(0.25) * ((v[0] + v[1]) + (v[2] + v[3]));
+#pragma unroll
+			for (int l = 0; l < 4; l++)
+				t[l] = v[l] - s;
+#pragma unroll
+			for (int k = 0; k < 3; k++)
+				cd[k] = d == 0 ? cod[0][k] : (d == 1 ? cod[1][k] : cod[2][k]);
+			p1_weak_derivative<T>(cd, v, t, o[h]);
+		}
+#pragma unroll
+		for (int i = 0; i < 10; i++)
+			R[i] = X == 0 ? o[0][i] - o[1][i] : o[1][i] - o[0][i];
+	} else {
+		const T sgn = X == 0 ? T(1) : T(-1);
+#pragma unroll
+		for (int i = 0; i < 10; i++)
+			R[i] = sgn * (sX[((fa * 2 + 1) * 10 + i) * P + lane] - sX[((fb * 2 + 0) * 10 + i) * P + lane]);
+	}
 #pragma unroll
 	for (int f = 0; f < 4; f++) {
 		T Fc[6];
@@ -439,11 +461,28 @@ __global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	T *sX = reinterpret_cast<T *>(smem_raw); // [120][P]
-	T *sF = sX + 120 * Rk3Smem<T>::P; // [144][P]
+	T *sF = FACT ? sX : sX + 120 * Rk3Smem<T>::P; // [144][P] (FACT: no sX)
 	const long long tile = blockIdx.x;
 	const int lane = threadIdx.x & 31;
 	const long long e = tile * 32 + lane;
 	const long long ec = e < p.ne ? e : p.ne - 1;
+	// the tile that starts on this SM about one CTA lifetime from now (l2_ahead
+	// = resident CTAs on the GPU): its state, k2, geometry and neighbour rows
+	// into L2, so that its first loads are L2 hits
+	if (threadIdx.x == 0 && p.l2_ahead > 0) {
+		const long long tn = tile + p.l2_ahead;
+		const long long nt = (p.ne + 31) / 32;
+		if (tn < nt) {
+			const unsigned wb = 60 * 32 * sizeof(T);
+			prefetch_l2(p.w_in + tn * 60 * 32, wb);
+			if (!p.stage0)
+				prefetch_l2(p.k2 + tn * 60 * 32, wb);
+			prefetch_l2(p.geom + tn * 10 * 32, 10 * 32 * sizeof(T));
+			const unsigned nbb = (unsigned)((p.ne - tn * 32 < 32 ? p.ne - tn * 32 : 32) * 16);
+			prefetch_l2(p.nb + tn * 32 * 4, nbb);
+			prefetch_l2(p.perm + tn * 32 * 4, nbb);
+		}
+	}
 	const T *Wt = p.w_in + tile * 60 * 32 + lane;
 	rk3_tile<T, SPARSE, FACT, PF, METAL>(p, tile, Wt, p.geom + tile * 10 * 32 + lane, p.k2 + tile * 60 * 32 + lane,
 										 reinterpret_cast<const int4 *>(p.nb) + ec,
@@ -536,14 +575,20 @@ bool rk3_tables_standard_faces(const gdn_cuda_tables *t)
 			return _rc;                                                                                            \
 	} while (0)
 
+template <typename T, bool FA>
+constexpr int rk3_smem_bytes()
+{
+	return FA ? Rk3Smem<T>::bytes_fact : Rk3Smem<T>::bytes;
+}
+
 template <typename T, bool SP, bool FA, bool METAL>
 static int prepare_rk3_one()
 {
 	typedef Rk3Variants<T> V;
 	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, FA, V::lo, V::pf_lo, METAL>,
-									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, rk3_smem_bytes<T, FA>()));
 	GDN_CUDA_TRY(cudaFuncSetAttribute(rk3_stage_kernel<T, SP, FA, V::hi, V::pf_hi, METAL>,
-									  cudaFuncAttributeMaxDynamicSharedMemorySize, Rk3Smem<T>::bytes));
+									  cudaFuncAttributeMaxDynamicSharedMemorySize, rk3_smem_bytes<T, FA>()));
 	return GDN_CUDA_OK;
 }
 
@@ -560,11 +605,14 @@ int prepare_rk3()
 }
 
 template <typename T, bool SP, bool FA, bool METAL>
-static void launch_rk3_one(const Rk3Params<T> &p, int variant, cudaStream_t s)
+static void launch_rk3_one(const Rk3Params<T> &pin, int variant, cudaStream_t s)
 {
 	typedef Rk3Variants<T> V;
+	Rk3Params<T> p = pin;
+	// L2 prefetch distance: the CTAs resident on the GPU at this variant's cap
+	p.l2_ahead = p.l2_ahead ? p.num_sms * (variant == 0 ? V::lo : V::hi) : 0;
 	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
-	const int sm = Rk3Smem<T>::bytes;
+	const int sm = rk3_smem_bytes<T, FA>();
 	if (variant == 0)
 		rk3_stage_kernel<T, SP, FA, V::lo, V::pf_lo, METAL><<<nblk, kRk3Threads, sm, s>>>(p);
 	else
