@@ -225,6 +225,12 @@ static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
 	for (int l = 0; l < 4; l++)
 		for (int j = 0; j < 10; j++)
 			o.Q4[l][j] = (T)q4[l][j];
+	double qs[6], ms[7];
+	rk3_sym_coeffs(t, qs, ms);
+	for (int k = 0; k < 6; k++)
+		o.q4_sym[k] = (T)qs[k];
+	for (int k = 0; k < 7; k++)
+		o.minv_sym[k] = (T)ms[k];
 	o.n3scale = (T)(t->ref_normal[3][0] * std::sqrt(3.0));
 	for (int f = 0; f < 4; f++) {
 		for (int k = 0; k < 3; k++)

@@ -39,6 +39,13 @@ struct Tables {
 	// Q4[l][j] = 4 int lambda_l phi_j (lambda_l the P1 barycentric basis):
 	// D[k] = G_k (Q4 / 4) with G_k the P1 coefficients of d_k(phi_i)
 	T Q4[4][NQN];
+	// The same Q4 and Minv through their tetrahedral symmetry (rk3_sym_coeffs):
+	// an entry depends only on how its two nodes sit (same vertex, two vertices,
+	// a vertex on / off an edge, same edge, edges sharing a vertex, opposite
+	// edges), so a product needs the vertex sum, the edge sum and the sum over
+	// the edges at each vertex plus a few coefficients.
+	T q4_sym[6];
+	T minv_sym[7];
 	T Minv[NQN][NQN];
 	T M[NQN][NQN];
 	T S[NQV][NQV];
