@@ -225,8 +225,10 @@ static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
 	for (int l = 0; l < 4; l++)
 		for (int j = 0; j < 10; j++)
 			o.Q4[l][j] = (T)q4[l][j];
-	double qs[6], ms[7];
-	rk3_sym_coeffs(t, qs, ms);
+	double qs[6], ms[7], ss[5];
+	rk3_sym_coeffs(t, qs, ms, ss);
+	for (int k = 0; k < 5; k++)
+		o.s_sym[k] = (T)ss[k];
 	for (int k = 0; k < 6; k++)
 		o.q4_sym[k] = (T)qs[k];
 	for (int k = 0; k < 7; k++)

@@ -46,6 +46,10 @@ struct Tables {
 	// the edges at each vertex plus a few coefficients.
 	T q4_sym[6];
 	T minv_sym[7];
+	// the P2 triangle face mass S the same way: vertex row (s_vv - s_vv')
+	// F_i + s_vv' (sum of vertex F) + s_ve F_opposite-edge; edge row (s_ee -
+	// s_ee') F_e + s_ee' (sum of edge F) + s_ve F_opposite-vertex
+	T s_sym[5];
 	T Minv[NQN][NQN];
 	T M[NQN][NQN];
 	T S[NQV][NQV];

@@ -45,7 +45,7 @@ struct Rk3Params {
 bool rk3_tables_sparse(const gdn_cuda_tables *t);
 bool rk3_tables_factor(const gdn_cuda_tables *t);
 void rk3_q4(const gdn_cuda_tables *t, double q4[4][10]);
-void rk3_sym_coeffs(const gdn_cuda_tables *t, double q4_sym[6], double minv_sym[7]);
+void rk3_sym_coeffs(const gdn_cuda_tables *t, double q4_sym[6], double minv_sym[7], double s_sym[5]);
 bool rk3_tables_standard_faces(const gdn_cuda_tables *t);
 
 // variant 0 / 1: the stage kernel compiled for fewer / more resident CTAs per

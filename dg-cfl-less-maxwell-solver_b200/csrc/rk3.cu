@@ -476,14 +476,26 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 #pragma unroll
 		for (int jj = 0; jj < 6; jj++)
 			Fc[jj] = sF[((f * 6 + jj) * 6 + c) * P + lane];
+		if (FACT) {
+			// S Fc through the triangle's symmetry (s_sym)
+			const T bv = tb.s_sym[1] * ((Fc[0] + Fc[1]) + Fc[2]);
+			const T be = tb.s_sym[4] * ((Fc[3] + Fc[4]) + Fc[5]);
 #pragma unroll
-		for (int ii = 0; ii < 6; ii++) {
-			T acc = T(0);
+			for (int ii = 0; ii < 3; ii++)
+				R[f2n(f, ii)] += bv + tb.s_sym[0] * Fc[ii] + tb.s_sym[2] * Fc[3 + (ii + 1) % 3];
 #pragma unroll
-			for (int jj = 0; jj < 6; jj++)
-				if (!SPARSE || (smask(ii) >> jj & 1))
-					acc += tb.S[ii][jj] * Fc[jj];
-			R[f2n(f, ii)] += acc;
+			for (int k = 0; k < 3; k++)
+				R[f2n(f, 3 + k)] += be + tb.s_sym[3] * Fc[3 + k] + tb.s_sym[2] * Fc[(k + 2) % 3];
+		} else {
+#pragma unroll
+			for (int ii = 0; ii < 6; ii++) {
+				T acc = T(0);
+#pragma unroll
+				for (int jj = 0; jj < 6; jj++)
+					if (!SPARSE || (smask(ii) >> jj & 1))
+						acc += tb.S[ii][jj] * Fc[jj];
+				R[f2n(f, ii)] += acc;
+			}
 		}
 	}
 	const T A = (T)p.A, B = (T)p.B;
@@ -588,8 +600,14 @@ static int node_pair_kind(int i, int j)
 
 // Coefficients of q4_apply_sym and lift_minv_sym from one representative
 // entry per kind (rk3_tables_factor checks that every entry equals its kind's).
-void rk3_sym_coeffs(const gdn_cuda_tables *t, double q4_sym[6], double minv_sym[7])
+void rk3_sym_coeffs(const gdn_cuda_tables *t, double q4_sym[6], double minv_sym[7], double s_sym[5])
 {
+	const double(*S)[6] = t->face_scal; // face nodes: vertices 0-2, edges 01, 12, 20
+	s_sym[0] = S[0][0] - S[0][1];
+	s_sym[1] = S[0][1];
+	s_sym[2] = S[0][4]; // vertex 0 and its opposite edge 12
+	s_sym[3] = S[3][3] - S[3][4];
+	s_sym[4] = S[3][4];
 	double q4[4][10];
 	rk3_q4(t, q4);
 	const double qa = q4[0][1], qb = q4[0][4], qc = q4[0][5]; // edge 4 = 0-1, edge 5 = 1-2
@@ -634,6 +652,27 @@ static bool rk3_tables_symmetric(const gdn_cuda_tables *t)
 		for (int j = 0; j < 10; j++)
 			if (!(std::fabs(M[i][j] - mrep[node_pair_kind(i, j)]) <= 1e-15 * mmax))
 				return false;
+	// face mass: kinds on the P2 triangle (face-local vertex i is opposite the
+	// edge 3 + (i + 1) % 3); a vertex and an edge through it: structural zero
+	const double(*S)[6] = t->face_scal;
+	double smax = 0.0;
+	for (int i = 0; i < 6; i++)
+		for (int j = 0; j < 6; j++)
+			smax = std::fmax(smax, std::fabs(S[i][j]));
+	for (int i = 0; i < 6; i++)
+		for (int j = 0; j < 6; j++) {
+			double rep;
+			if (i < 3 && j < 3)
+				rep = i == j ? S[0][0] : S[0][1];
+			else if (i >= 3 && j >= 3)
+				rep = i == j ? S[3][3] : S[3][4];
+			else {
+				const int v = i < 3 ? i : j, ed = i < 3 ? j : i;
+				rep = ed == 3 + (v + 1) % 3 ? S[0][4] : 0.0;
+			}
+			if (!(std::fabs(S[i][j] - rep) <= 1e-15 * smax))
+				return false;
+		}
 	return true;
 }
 
