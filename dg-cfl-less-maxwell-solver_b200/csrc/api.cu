@@ -427,6 +427,7 @@ static int autotune_rk3(gdn_cuda_handle *h)
 	p.sparse = h->rk3_sparse;
 	p.fact = h->rk3_fact;
 	p.num_sms = h->num_sms;
+	p.idx32 = (h->ne + 31) / 32 * 1920 <= 0xffffffffLL;
 	p.l2_ahead = 1;
 	p.bc_metal = h->bc_metal;
 	cudaEvent_t ev[2];
@@ -939,6 +940,7 @@ static int rk3_enqueue(gdn_cuda_handle *h, int &cur, long long &nlaunch)
 		p.sparse = h->rk3_sparse;
 		p.fact = h->rk3_fact;
 		p.num_sms = h->num_sms;
+		p.idx32 = (h->ne + 31) / 32 * 1920 <= 0xffffffffLL;
 		p.l2_ahead = 1;
 		p.bc_metal = h->bc_metal;
 		if (h->nbf > 0) {

@@ -39,6 +39,7 @@ struct Rk3Params {
 	int fact; // the derivative tables factor through the P1 basis (rk3_tables_factor)
 	int bc_metal; // boundary faces take the metal flux (-n x H_L, 0)
 	int num_sms; // SMs of the device
+	int idx32; // every tiled state offset fits 32 bits (ntiles * 1920 < 2^32)
 	int l2_ahead; // nonzero: prefetch into L2 the tile this many CTAs ahead (set per variant at launch)
 };
 

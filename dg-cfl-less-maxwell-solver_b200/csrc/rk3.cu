@@ -334,18 +334,22 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 #pragma unroll
 			for (int f = 0; f < 4; f++) {
 				const int nbv = nbk[f];
-				const T *g;
-				int st;
+				T *d = sF + ((f * 6 + warp) * 6) * P + lane;
+				// constant strides in each branch, so the six copies use
+				// immediate offsets; 32-bit tile offsets when the state fits
 				if (nbv >= 0) {
-					g = p.w_in + rk3_tix(nbv, ((pmk[f] >> (4 * warp)) & 15) * 6);
-					st = 32;
-				} else {
-					g = p.btrace + ((long long)(-nbv - 1) * 6 + warp) * 6;
-					st = 1;
-				}
+					const unsigned qn = ((unsigned)pmk[f] >> (4 * warp)) & 15u;
+					const T *g = p.idx32 ? p.w_in + (((unsigned)nbv >> 5) * 1920u + qn * 192u + ((unsigned)nbv & 31u))
+										 : p.w_in + rk3_tix(nbv, (int)qn * 6);
 #pragma unroll
-				for (int cc = 0; cc < 6; cc++)
-					cp_async_value<T>(sF + ((f * 6 + warp) * 6 + cc) * P + lane, g + cc * st);
+					for (int cc = 0; cc < 6; cc++)
+						cp_async_value<T>(d + cc * P, g + cc * 32);
+				} else {
+					const T *g = p.btrace + ((long long)(-nbv - 1) * 6 + warp) * 6;
+#pragma unroll
+					for (int cc = 0; cc < 6; cc++)
+						cp_async_value<T>(d + cc * P, g + cc);
+				}
 			}
 		}
 #pragma unroll

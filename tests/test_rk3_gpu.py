@@ -208,3 +208,24 @@ def test_rk3_variants_metal_boundary(variant):
     s.close()
     rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
     assert rel <= FP64_RTOL, rel
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.FP32])
+def test_rk3_table_product_path_matches_reference(precision):
+    """Tables without the tetrahedral symmetry the factored kernel relies on
+    (one inverse-mass pair moved by 1e-13 of the largest entry, far below the
+    FP64 tolerance but above the attach check's 1e-15) run the table-product
+    kernel (structural zeros of D_k and of the face mass removed, derivatives
+    exchanged through shared memory): still the reference's result."""
+    mesh, dt, r = _ref15("plane")
+    t = capi.t10_tables()
+    d = 1e-13 * 600.0
+    t.inv_mass[0][1] += d
+    t.inv_mass[1][0] += d
+    data = capi.plane_data(khat=(0.6, 0.8, 0.0), kmag=4 * np.pi, pol=(0, 0, 1))
+    for v in (1, 2):
+        s = capi.Solver(mesh, capi.SCHEME_RK3, data, dt, precision=precision, tables=t, rk3_variant=v)
+        wn, _, _ = s.solve(20)
+        s.close()
+        rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+        assert rel <= (FP64_RTOL if precision == capi.FP64 else 2e-5), (v, rel)
