@@ -173,3 +173,67 @@ def test_convergence_drivers_validate_before_touching_the_device():
     with pytest.raises(capi.GdnError) as ex:
         capi.time_convergence(m, capi.SCHEME_RK3, capi.plane_data(), 0.1, 1.0, 0)
     assert ex.value.code == capi.ERR_INVALID
+
+
+def _p2_sums(x):
+    edges = [(0, 1), (1, 2), (0, 2), (0, 3), (1, 3), (2, 3)]
+    sv, se = x[:4].sum(), x[4:].sum()
+    ev = np.array([sum(x[4 + e] for e, (a, b) in enumerate(edges) if l in (a, b)) for l in range(4)])
+    return sv, se, ev, edges
+
+
+@pytest.mark.parametrize("which", ["ours", "reference"])
+def test_symmetric_table_forms_reproduce_the_table_products(which):
+    """The factored RK3 kernel replaces three table products by sums over the
+    P2 tetrahedron's symmetry (q4_apply_sym, lift_minv_sym, the face-mass lift)
+    and the volume derivative by the P1-basis form (p1_weak_derivative).  The
+    same algebra in numpy, against the dense products of the tables handed to
+    attach (ours and the reference's)."""
+    from oracle import ref
+    if which == "ours":
+        t = capi.tables_as_numpy(capi.t10_tables())
+        D = t["internal"].reshape(10, 10, 3)
+        M, Mi, S = t["mass"].reshape(10, 10), t["inv_mass"].reshape(10, 10), t["face_scal"].reshape(6, 6)
+    else:
+        t = ref.t10_tables()
+        D, M, Mi, S = t["internal"], t["mass"], t["inv_mass"], t["face_scal"]
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(10)
+    sv, se, ev, edges = _p2_sums(x)
+    # Q4 = 4 Lambda M (lambda_l interpolated exactly in P2), vertex diagonal zero
+    Lam = np.zeros((4, 10))
+    for l in range(4):
+        Lam[l, l] = 1.0
+    for e, (a, b) in enumerate(edges):
+        Lam[a, 4 + e] = Lam[b, 4 + e] = 0.5
+    Q4 = 4.0 * Lam @ M
+    for l in range(4):
+        Q4[l, l] = 0.0
+    qa, qb, qc = Q4[0, 1], Q4[0, 4], Q4[0, 5]
+    v = (qa * sv + qc * se) - qa * x[:4] + (qb - qc) * ev
+    assert np.abs(v - Q4 @ x).max() <= 1e-15 * np.abs(Q4 @ x).max() * 10
+    assert abs((0.75 * qa * sv + 0.5 * (qb + qc) * se) - v.sum() / 4) <= 1e-15
+    # weak derivative along g through the P1 basis == sum_k g_k D_k w
+    g3 = rng.standard_normal(3)
+    g = np.array([-g3.sum(), *g3])
+    t4 = v - v.sum() / 4
+    out = np.concatenate([g * t4, [g[a] * v[b] + g[b] * v[a] for a, b in edges]])
+    dense = sum(g3[k] * (D[:, :, k] @ x) for k in range(3))
+    assert np.abs(out - dense).max() <= 1e-14 * np.abs(dense).max()
+    # Minv R through the symmetry
+    m = [Mi[0, 1], Mi[0, 5], Mi[4, 9], Mi[0, 0] - Mi[0, 1], Mi[0, 4] - Mi[0, 5],
+         Mi[4, 4] - 2 * Mi[4, 5] + Mi[4, 9], Mi[4, 5] - Mi[4, 9]]
+    bv, be = m[0] * sv + m[1] * se, m[1] * sv + m[2] * se
+    dw = np.concatenate([bv + m[3] * x[:4] + m[4] * ev,
+                         [be + m[4] * (x[a] + x[b]) + m[5] * x[4 + e] + m[6] * (ev[a] + ev[b])
+                          for e, (a, b) in enumerate(edges)]])
+    assert np.abs(dw - Mi @ x).max() <= 1e-13 * np.abs(Mi @ x).max()
+    # face mass on the triangle (vertices 0-2, edges 01, 12, 20)
+    F = rng.standard_normal(6)
+    s = [S[0, 0] - S[0, 1], S[0, 1], S[0, 4], S[3, 3] - S[3, 4], S[3, 4]]
+    fo = np.zeros(6)
+    for i in range(3):
+        fo[i] = s[1] * F[:3].sum() + s[0] * F[i] + s[2] * F[3 + (i + 1) % 3]
+    for k in range(3):
+        fo[3 + k] = s[4] * F[3:].sum() + s[3] * F[3 + k] + s[2] * F[(k + 2) % 3]
+    assert np.abs(fo - S @ F).max() <= 1e-15 * np.abs(S @ F).max() * 10
