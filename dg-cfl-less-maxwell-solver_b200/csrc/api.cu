@@ -208,15 +208,8 @@ static void fill_tables(const gdn_cuda_tables *t, Tables<T> &o)
 	for (int i = 0; i < 6; i++)
 		for (int j = 0; j < 6; j++)
 			o.S[i][j] = (T)t->face_scal[i][j];
-	for (int i = 0; i < 10; i++)
-		for (int j = 0; j < 10; j++) {
-			o.D01[i][j].x = o.D[0][i][j];
-			o.D01[i][j].y = o.D[1][i][j];
-		}
 	for (int m = 0; m < 5; m++)
 		for (int j = 0; j < 10; j++) {
-			o.D2p[m][j].x = o.D[2][2 * m][j];
-			o.D2p[m][j].y = o.D[2][2 * m + 1][j];
 			o.MinvP[m][j].x = o.Minv[2 * m][j];
 			o.MinvP[m][j].y = o.Minv[2 * m + 1][j];
 		}

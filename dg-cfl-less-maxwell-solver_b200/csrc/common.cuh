@@ -27,13 +27,10 @@ struct Vec2<double> {
 
 // Reference-element tables, in constant memory so that warp-uniform indices
 // broadcast.  D[k][i][j] = int d_k(phi_i) phi_j (t10_internal_ref[i][j][k]).
-// The *p / D01 arrays hold the same coefficients as adjacent pairs for the
-// packed FP32x2 FMA: D01[i][j] = (D[0][i][j], D[1][i][j]),
-// D2p[m][j] = (D[2][2m][j], D[2][2m+1][j]), MinvP[m][j] = (Minv[2m][j], Minv[2m+1][j]).
+// MinvP[m][j] = (Minv[2m][j], Minv[2m+1][j]): row pairs for the packed FP32x2
+// FMA of the table-product RK3 path.
 template <typename T>
 struct Tables {
-	typename Vec2<T>::type D01[NQN][NQN];
-	typename Vec2<T>::type D2p[NQN / 2][NQN];
 	typename Vec2<T>::type MinvP[NQN / 2][NQN];
 	T D[3][NQN][NQN];
 	// Q4[l][j] = 4 int lambda_l phi_j (lambda_l the P1 barycentric basis):
