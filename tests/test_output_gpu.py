@@ -59,3 +59,34 @@ def test_save_xdmf_writes_the_reference_content(tmp_path, scheme, nb_v):
     seeks = [int(d.get("Seek")) for d in grid.findall("Attribute/DataItem") if d.get("Seek") is not None]
     assert seeks[:m] == [im * nq * 8 for im in range(m)]
     assert os.path.basename(base) + "_data_0003.bin" in ET.tostring(grid).decode()
+
+
+@pytest.mark.parametrize("scheme", [capi.SCHEME_RK3, capi.SCHEME_KINETIC])
+def test_save_xdmf_of_a_batch_instance_equals_its_single_solve(tmp_path, scheme):
+    """The files written for instance i of a batch handle (instance-local
+    connectivity and nodes, its own state and time) are byte-identical to
+    those of the same instance solved alone."""
+    specs = [(2, 0.1, 1), (3, 0.0, 2), (2, 0.15, 3)]
+    meshes, datas, dts = [], [], []
+    for k, (n, jitter, seed) in enumerate(specs):
+        c, e = kuhn.kuhn_cube(n, jitter, seed=seed)
+        meshes.append(capi.mesh_build(c, e))
+        datas.append(capi.plane_data(kmag=2 * np.pi * (1 + k)))
+        dts.append((1 if scheme == capi.SCHEME_RK3 else 10) * 0.3 * meshes[-1].hmin())
+    b = capi.BatchSolver(meshes, datas, dts, scheme=scheme, rk3_variant=1)
+    b.solve(4)
+    for i in (1, 2):
+        b.save_xdmf(str(tmp_path / ("batch%d" % i)), 4, instance=i)
+    b.close()
+    for i in (1, 2):
+        s = capi.Solver(meshes[i], scheme, datas[i], dts[i], rk3_variant=1)
+        s.solve(4)
+        s.save_xdmf(str(tmp_path / ("single%d" % i)), 4)
+        s.close()
+        for suffix in ("_mesh_conn.bin", "_mesh_nodes.bin", "_data_0004.bin"):
+            a = (tmp_path / ("batch%d%s" % (i, suffix))).read_bytes()
+            o = (tmp_path / ("single%d%s" % (i, suffix))).read_bytes()
+            assert a == o, (i, suffix)
+        xa = (tmp_path / ("batch%d_simulation_0004.xmf" % i)).read_text().replace("batch%d" % i, "X")
+        xo = (tmp_path / ("single%d_simulation_0004.xmf" % i)).read_text().replace("single%d" % i, "X")
+        assert xa == xo, i
