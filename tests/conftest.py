@@ -12,7 +12,6 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG_DIR = os.path.join(ROOT, "dg-cfl-less-maxwell-solver_b200")
-REFERENCE_TREE = "/root/reference"
 
 
 def load_package():

@@ -45,9 +45,9 @@ def test_kinetic_d3q6_plane_fp64_matches_reference():
     assert rel <= 1e-12, rel
 
 
-def test_kinetic_cfg2_cavity_16_fp64_matches_reference():
-    """16^3 x 6 tets, cavity, dt = 10 x the RK3 CFL
-    step, 100 steps, d3q4."""
+def test_kinetic_cavity_16_fp64_matches_reference():
+    """The plain CFL-less relaxation workload: 16^3 x 6 tets, PEC cavity mode,
+    dt = 10 x the RK3 CFL step, 100 steps, d3q4."""
     wn, t, err, r, levels = _pair(16, 0.0, 100, 10)
     rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
     assert rel <= 1e-12, rel
