@@ -97,6 +97,8 @@ def test_null_handle_calls_fail_cleanly():
     d = C.c_double()
     assert L.gdn_cuda_error_l2(None, C.byref(d)) == capi.ERR_INVALID
     assert b"bad arguments" in L.gdn_cuda_last_error()
+    assert L.gdn_cuda_save_xdmf(None, 0, b"/nonexistent/x", 0) == capi.ERR_INVALID
+    assert b"save_xdmf: bad arguments" in L.gdn_cuda_last_error()
 
 
 @pytest.mark.parametrize("n,jitter", [(1, 0.0), (3, 0.0), (4, 0.15), (6, 0.3)])
