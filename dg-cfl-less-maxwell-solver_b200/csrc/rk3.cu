@@ -521,17 +521,11 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 }
 
 // One CTA per tile, everything read from global memory.
-// register cap for MINB resident CTAs of kRk3Threads threads per SM (64 K
-// registers, allocated per thread in multiples of 8); stated as __maxnreg__
-// because with __launch_bounds__(threads, MINB) ptxas stopped at 96 registers
-// for 3 FP64 CTAs and spilled
-constexpr int rk3_max_regs(int minb)
-{
-	return (65536 / (minb * kRk3Threads)) / 8 * 8;
-}
-
+// MINB resident CTAs per SM: ptxas derives the register cap, including the
+// split of the register file between the SM's four schedulers (18 warps of 3
+// CTAs leave 5 warps on one scheduler: 96 registers, not 65536 / 576)
 template <typename T, bool SPARSE, bool FACT, int MINB, int PF, bool METAL>
-__global__ void __maxnreg__(rk3_max_regs(MINB)) rk3_stage_kernel(Rk3Params<T> p)
+__global__ void __launch_bounds__(kRk3Threads, MINB) rk3_stage_kernel(Rk3Params<T> p)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	T *sX = reinterpret_cast<T *>(smem_raw); // [120][P]
