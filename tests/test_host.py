@@ -239,3 +239,33 @@ def test_symmetric_table_forms_reproduce_the_table_products(which):
     for k in range(3):
         fo[3 + k] = s[4] * F[3:].sum() + s[3] * F[3 + k] + s[2] * F[(k + 2) % 3]
     assert np.abs(fo - S @ F).max() <= 1e-15 * np.abs(S @ F).max() * 10
+
+
+def _rk3_tix(e, k):
+    return ((e >> 5) * 60 + k) * 32 + (e & 31)
+
+
+@pytest.mark.parametrize("ne", [1, 31, 32, 33, 1000, 5308416, 71_582_784])
+def test_rk3_gather_and_prefetch_offsets_stay_in_bounds(ne):
+    """Index arithmetic of the RK3 stage kernel, restated: the 32-bit
+    neighbour-trace offset used when the tiled state fits 32 bits equals the
+    64-bit tiled index, every trace read (6 fields, stride 32) lies inside the
+    ntiles * 1920 values allocated, and the L2 prefetch of a tile covers only
+    allocated rows (state / k2 / geometry padded to whole tiles, neighbour and
+    permutation rows only for live elements)."""
+    nt = (ne + 31) // 32
+    idx32 = nt * 1920 <= 0xFFFFFFFF
+    rng = np.random.default_rng(ne)
+    nbv = np.unique(np.concatenate([[0, ne - 1], rng.integers(0, ne, 200)]))
+    for qn in range(10):
+        k64 = np.array([_rk3_tix(int(v), qn * 6) for v in nbv])
+        assert (k64 + 5 * 32 < nt * 1920).all()
+        if idx32:
+            k32 = ((nbv.astype(np.uint64) >> 5) * 1920 + qn * 192 + (nbv.astype(np.uint64) & 31)) & 0xFFFFFFFF
+            assert np.array_equal(k32.astype(np.int64), k64)
+    assert idx32 == (ne <= 71_582_784)
+    for tn in (0, nt - 1):
+        live = min(32, ne - tn * 32)
+        assert 1 <= live <= 32
+        assert tn * 1920 + 1920 <= nt * 1920 and tn * 320 + 320 <= nt * 320
+        assert tn * 32 * 4 + live * 4 <= 4 * ne  # nb / perm ints (16 bytes per element)
