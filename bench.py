@@ -215,8 +215,10 @@ def cpu_reference_kinetic_sample(steps=10, n=KIN_CPU_N):
         r = rm.run(ref.SCHEME_D3Q4, ref.make_data(kind=ref.DATA_CAVITY), dt, steps)
     dofs = 10 * len(e) * 24 * steps
     return {"value": dofs / r["cpu_run"], "unit": "DoF-updates/s", "cores": threads, "kind": "reference",
-            "sample": "reference dg_solve_relaxation (oracle/_ref, -O3 -fopenmp, exact sparse LU shim) on a "
-                      "%d^3x6 = %d-tet cavity mesh, d3q4, %dx CFL, %d steps, time loop only"
+            "sample": "reference dg_solve_relaxation (oracle/_ref, -O3 -fopenmp) on a %d^3x6 = %d-tet cavity "
+                      "mesh, d3q4, %dx CFL, %d steps, time loop only; its sparse solves run the oracle's "
+                      "block-triangular direct LU (oracle/shim/sparse_shim.c), not SuiteSparse KLU, which "
+                      "is not installed"
                       % (n, len(e), KIN_MULT, steps)}
 
 

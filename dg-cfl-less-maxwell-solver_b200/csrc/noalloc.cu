@@ -1,11 +1,10 @@
 // gdn_cuda_error_l2_noalloc: the FP64 L2 error norm of an RK3 state for
 // callers that cannot allocate device memory.
 //
-// Some callers of this library cannot call cudaMalloc: code that runs while a
-// stream is being captured into a CUDA graph, hosts whose device memory is
-// owned by another allocator or a fixed budget set at start-up, and
-// long-running services that must not allocate after initialisation.  They
-// already hold their inputs and outputs; what they cannot provide is the
+// Some callers of this library cannot call cudaMalloc: hosts whose device
+// memory is owned by another allocator or by a fixed budget set at start-up,
+// and long-running services that must not allocate after initialisation.
+// They already hold their inputs and outputs; what they cannot provide is the
 // library's own scratch.  This entry point keeps that scratch in a
 // fixed-size array that lives in the library's device image: every GPU that
 // loads the library holds it (about 192 KB) until the process exits.
@@ -14,10 +13,16 @@
 //   - at most kMaxBlocks x kBlockElems = 8,388,608 elements per call; larger
 //     meshes are rejected with GDN_CUDA_ERR_INVALID;
 //   - every call shares the one array per device and it keeps the last
-//     call's contents: calls that overlap on the GPU (two streams, two host
+//     call's contents (each call overwrites every slot it reads, so nothing
+//     needs clearing): calls that overlap on the GPU (two streams, two host
 //     threads) race and must be serialised by the caller;
-//   - the first call on a device looks up the array's device address on that
-//     device; make that first call before any stream capture begins.
+//   - the call synchronises its stream before it returns, so the result is
+//     in the caller's host variable on return;
+//   - the first call on a device (that device current, in its primary
+//     context) looks up the array's device address there and keeps it: make
+//     that first call before any stream capture begins; the kept address does
+//     not survive cudaDeviceReset.
+#include <atomic>
 #include <cstdio>
 
 #include "common.cuh"
@@ -99,8 +104,10 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_error_final(int nblk,
 	}
 }
 
-// device address of g_noalloc_scratch, looked up once per device
-static void *g_noalloc_ptr[256];
+// device address of g_noalloc_scratch, looked up once per device (atomic:
+// first calls from several host threads may race to fill a slot, and each
+// stores the same address)
+static std::atomic<void *> g_noalloc_ptr[256];
 
 } // namespace gdn
 
@@ -125,14 +132,16 @@ extern "C" int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, con
 	GDN_CUDA_TRY(cudaGetDevice(&dev));
 	if (dev < 0 || dev >= 256)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "error_l2_noalloc: device ordinal out of range");
-	if (!g_noalloc_ptr[dev]) {
+	void *cached = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+	if (!cached) {
 		void *ptr = nullptr;
 		cudaError_t rc = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
 		if (rc != cudaSuccess || !ptr)
 			return gdn_cuda_fail(rc, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-		g_noalloc_ptr[dev] = ptr;
+		g_noalloc_ptr[dev].store(ptr, std::memory_order_release);
+		cached = ptr;
 	}
-	double *scratch = static_cast<double *>(g_noalloc_ptr[dev]);
+	double *scratch = static_cast<double *>(cached);
 	Data d;
 	d.kind = data->kind;
 	for (int c = 0; c < 3; c++) {

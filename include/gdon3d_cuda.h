@@ -232,18 +232,27 @@ int gdn_cuda_error_l2(gdn_cuda_handle *h, double *err);
 int gdn_cuda_error_l2_batch(gdn_cuda_handle *h, double *err);
 
 /* No counterpart in the reference.  The same norm as gdn_cuda_error_l2 for
- * callers that cannot allocate device memory (code running under stream
- * capture, hosts whose device memory belongs to another allocator or a fixed
- * start-up budget): it allocates nothing and uses a fixed scratch array of
- * about 192 KB that every GPU loading the library holds until exit.
- * Inputs are device pointers the caller owns: w[nbelems*10*6] (the RK3
- * volume state, reference layout), xyz[nbelems*10*3] (P2 node coordinates),
- * det[nbelems] (Jacobian determinants); wpg[10] is host memory; *err is
- * written on the host after `stream` (a cudaStream_t, NULL = legacy stream)
- * completes.  At most 8,388,608 elements (GDN_CUDA_ERR_INVALID beyond).  All
- * calls share the scratch: calls that overlap on the GPU race.  The first
- * call on a device resolves the scratch address and should come before any
- * stream capture. */
+ * callers that cannot allocate device memory (hosts whose device memory
+ * belongs to another allocator or to a fixed budget set at start-up,
+ * services that must not allocate after initialisation): it allocates
+ * nothing and uses a fixed scratch array of about 192 KB that every GPU
+ * loading the library holds until exit.
+ * Inputs are device pointers the caller owns, all FP64:
+ *   w[nbelems*10*6]    the RK3 volume state in the reference layout
+ *                      [element][node][component] (the first 60 * nbelems
+ *                      values of gdn_simulation.wn);
+ *   xyz[nbelems*10*3]  the coordinates of each element's 10 P2 nodes;
+ *   det[nbelems]       the Jacobian determinants, signed as the reference's
+ *                      geometry has them (positive for positively oriented
+ *                      tetrahedra), the same values gdn_cuda_error_l2 uses;
+ * wpg[10] and *err are host memory.  The call launches on `stream` (a
+ * cudaStream_t, NULL = legacy stream), then synchronises that stream before
+ * it returns: *err is valid on return.  At most 8,388,608 elements
+ * (GDN_CUDA_ERR_INVALID beyond).  All calls share the scratch array: calls
+ * that overlap on the GPU race.  The first call on a device (that device
+ * current, in its primary context) looks up the array's device address and
+ * keeps it; it should come before any stream capture, and the address does
+ * not survive cudaDeviceReset. */
 int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, const double *det, long long nbelems,
 							  const double *wpg, const gdn_cuda_data *data, double t, void *stream,
 							  double *err);

@@ -1,9 +1,11 @@
 """GPU: gdn_cuda_error_l2_noalloc, the allocation-free variant of the L2
-error norm, for callers that cannot call cudaMalloc (code under stream
-capture, hosts whose device memory belongs to another allocator or a fixed
-budget).  Its inputs are device buffers the caller owns (allocated here by the
-test, not by the library); its result must equal the handle-based
-gdn_cuda_error_l2 on the same state, on two calls in a row.
+error norm, for callers that cannot call cudaMalloc (hosts whose device memory
+belongs to another allocator or to a fixed budget set at start-up).  Its
+inputs are device buffers the caller owns (allocated here by the test, not by
+the library); its result must equal the handle-based gdn_cuda_error_l2 on the
+same state, on two calls in a row: on a mesh of one partial-sum block
+(1,296 elements) and on one of six blocks whose last block is partly filled
+(10,368 elements = 5 x 2,048 + 128).
 
 Kept in its own file, collected last, so that a run stopping at the first
 failure has already run every other test."""
@@ -23,9 +25,10 @@ def _dev(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
 
 
-def test_error_l2_noalloc_matches_error_l2_twice():
+@pytest.mark.parametrize("n", [6, 12])
+def test_error_l2_noalloc_matches_error_l2_twice(n):
     import torch
-    coords, e2n = kuhn.kuhn_cube(6, 0.1, seed=4)
+    coords, e2n = kuhn.kuhn_cube(n, 0.1, seed=4)
     mesh = capi.mesh_build(coords, e2n)
     ne = mesh.nbelems
     k = np.array([0.3, -0.4, 0.5])
