@@ -320,25 +320,51 @@ def main():
     ap.add_argument("--only", default="all",
                     help="profiling aid: comma-separated variants to run (rk3: fp64,fp32; kinetic: "
                          "fp64,fp32,fp32_refine1,fp32_refine2,bf16)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="rk3: print the 96^3 line without the kinetic precision study and the batch")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"rk3": 50, "kinetic": KIN_STEPS, "batched": BATCH_RK3_STEPS}[args.workload]
     if args.impl == "reference":
         return run_reference_arm(args)
-    if args.workload == "batched":
+    with_all = args.workload == "rk3" and not args.headline_only and args.n is None
+    specs = built = None
+    if args.workload == "batched" or with_all:
         # meshes first, in spawned worker processes (no CUDA in them)
         specs = load_package().kuhn.uneven_plane_wave_batch(SEED, args.count)
         ctx = multiprocessing.get_context("spawn")
         with concurrent.futures.ProcessPoolExecutor(max_workers=min(32, os.cpu_count() or 1),
                                                     mp_context=ctx) as ex:
             built = list(ex.map(_build_instance_mesh, specs, chunksize=4))
-        env = Env(args)
-        rc = run_batched(args, env, specs, built)
+    env = Env(args)
+    if args.workload == "batched":
+        line = run_batched(args, env, specs, built)
+    elif args.workload == "kinetic":
+        line = run_kinetic(args, env)
     else:
-        env = Env(args)
-        rc = run_kinetic(args, env) if args.workload == "kinetic" else run_rk3(args, env)
+        line = run_rk3(args, env)
+        if with_all:
+            # configs 4 and 5 ride on the default line, each with its own
+            # clocks and roofline: the 64^3 kinetic precision study (100
+            # steps per variant) and the 256-instance uneven batch
+            kargs = argparse.Namespace(**vars(args))
+            kargs.steps = KIN_STEPS
+            kargs.n = None
+            kargs.only = "all"
+            line["kinetic_precision_study"] = _strip(run_kinetic(kargs, env))
+            line["batched_uneven_256"] = _strip(run_batched(args, env, specs, built))
+    if env.rank == 0:
+        print(json.dumps(line), flush=True)
     env.close()
-    return rc
+    return 0
+
+
+def _strip(line):
+    """A sub-benchmark's line as a key of the default line: its own metric,
+    value, config, roofline, clocks and variants, without the keys that only
+    the top-level line carries."""
+    return {k: v for k, v in line.items()
+            if k not in ("n_gpus", "vs_baseline", "e2e", "e2e_note", "data", "scaling", "higher_is_better")}
 
 
 def _wanted(args, name):
@@ -462,9 +488,7 @@ def run_rk3(args, env):
         "e2e": e2e,
         "cpu_baseline": cpu,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 
@@ -528,6 +552,7 @@ def run_kinetic(args, env):
         err = s.error_l2()
         wn = s.get_state()
         levels = s.num_levels
+        mode = s.kin_sweep_mode
         s.close()
         if vol is None:
             vol = np.zeros((24, len(wn) // 24), bool)
@@ -544,11 +569,28 @@ def run_kinetic(args, env):
         alg = kinetic_algorithmic_bytes(ne, b_s, b_g)
         achieved = alg / (ms * 1e-3) / 1e9
         res[name] = {"value": job_rate(env.world, dofs_per_step, ms * 1e-3), "ms_per_step": ms,
-                     "gpu_launches": launches, "levels": levels, "clocks": clk,
+                     "gpu_launches": launches, "levels": levels, "sweep_mode": mode, "clocks": clk,
                      "l2_rel_vs_fp64": rel, "l2_error_vs_analytic": err,
                      "roofline": {"bound": "hbm", "scope": "whole step vs the minimum traffic",
                                   "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                                   "peak_kind": peak_kind, "algorithmic_bytes_per_step": alg}}
+    # the three sweep-level groupings of the transport solve, timed alone
+    # (the variants above run the one the autotuner picked)
+    sweep_modes = {}
+    for name, prec in (("fp64", capi.FP64), ("fp32", capi.FP32)):
+        if not _wanted(args, name):
+            continue
+        sweep_modes[name] = {}
+        for mode, label in ((1, "level_launches"), (2, "cooperative_grid_barrier"), (3, "readiness_flags")):
+            s = capi.Solver(mesh, capi.SCHEME_KINETIC, data, dt, precision=prec, nb_v=4, device=env.local,
+                            kin_sweep=mode)
+            s.init()
+            s.advance(W)
+            s.init()
+            ms, launches, _ = _time_advance(env, s, min(K, 20), env.local)
+            s.close()
+            sweep_modes[name][label] = {"ms_per_step": ms / min(K, 20), "gpu_launches_per_step":
+                                        launches / min(K, 20)}
     if "fp64" in res:
         e64 = res["fp64"]["l2_error_vs_analytic"]
         for r in res.values():
@@ -577,13 +619,11 @@ def run_kinetic(args, env):
                    "l2_flush": "inputs larger than L2: %.2f GB of distributions" % (ne * 240 * 4 / 1e9),
                    "parallelism": "replicas" if env.world > 1 else "single-gpu"},
         "roofline": head["roofline"], "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
-        "variants": res, "e2e": None,
+        "variants": res, "sweep_modes": sweep_modes, "e2e": None,
         "e2e_note": "the end-to-end line is the default (rk3) workload's",
         "cpu_baseline": cpu,
     }
-    if env.rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_batched(args, env, specs, built):
@@ -640,6 +680,7 @@ def run_batched(args, env, specs, built):
     err_b = {"rk3": brk.error_l2_batch(), "kinetic": bkn.error_l2_batch()}
     tile = brk.rk3_variant
     levels = bkn.num_levels
+    kmode = bkn.kin_sweep_mode
     brk.close()
     bkn.close()
     value = job_rate(env.world, dofs_rk + dofs_kn, ms_batch * 1e-3)
@@ -684,6 +725,8 @@ def run_batched(args, env, specs, built):
                    "kinetic_elements": int(sum(ne[i] for i in kn)), "n_range": [8, 40], "jitter": 0.1,
                    "seed": SEED, "rk3_steps": BATCH_RK3_STEPS, "kinetic_steps": BATCH_KIN_STEPS,
                    "kinetic_cfl_multiple": BATCH_KIN_MULT, "rk3_variant_autotuned": tile,
+                   "kinetic_sweep_mode_autotuned": {1: "level_launches", 2: "cooperative_grid_barrier",
+                                                    3: "readiness_flags"}.get(kmode, kmode),
                    "kinetic_levels": levels, "attach_s": attach_s,
                    "precision": "FP32 state and arithmetic; FP64 setup and norms",
                    "l2_flush": "inputs larger than L2 (%.1f GB of FP32 RK3 state)"
@@ -701,9 +744,7 @@ def run_batched(args, env, specs, built):
         "e2e": None, "e2e_note": "the end-to-end line is the default (rk3) workload's",
         "cpu_baseline": None,
     }
-    if env.rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 if __name__ == "__main__":

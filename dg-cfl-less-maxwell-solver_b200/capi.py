@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "libgdon3d_cuda.so")
 
 OK = 0
 ERR_CUDA, ERR_INVALID, ERR_UNSUPPORTED, ERR_CYCLE, ERR_OOM, ERR_TIMEOUT, ERR_MESH = 1, 2, 3, 4, 5, 6, 7
-DATA_PLANE, DATA_CAVITY = 0, 1
+DATA_PLANE, DATA_CAVITY, DATA_STATIONARY = 0, 1, 2
 SCHEME_RK3, SCHEME_KINETIC = 0, 1
 BC_UPWIND, BC_METAL = 0, 1
 FP64, FP32, FP32_REFINE, BF16_STORE = 0, 1, 2, 3
@@ -79,7 +79,8 @@ EXPORTS = [
     "gdn_cuda_stream", "gdn_cuda_last_error", "gdn_cuda_error_l2_noalloc", "gdn_cuda_attach_batch",
     "gdn_cuda_error_l2_batch", "gdn_cuda_num_instances", "gdn_cuda_instance_info", "gdn_cuda_rk3_variant",
     "gdn_cuda_kin_sweep_mode", "gdn_cuda_time_convergence", "gdn_cuda_space_convergence",
-    "gdn_cuda_mesh_build_gpu", "gdn_cuda_save_xdmf",
+    "gdn_cuda_mesh_build_gpu", "gdn_cuda_save_xdmf", "gdn_cuda_eval_data",
+    "gdn_cuda_set_wait_limit",
 ]
 
 _lib = None
@@ -127,6 +128,8 @@ def lib():
     L.gdn_cuda_space_convergence.argtypes = [C.POINTER(C.POINTER(Mesh)), C.c_int, C.POINTER(Tables),
                                              C.POINTER(Model), C.POINTER(Data), C.POINTER(Config), C.c_double,
                                              C.c_double, C.c_int, dp, ip, dp, dp, dp]
+    L.gdn_cuda_set_wait_limit.argtypes = [vp, C.c_longlong]
+    L.gdn_cuda_eval_data.argtypes = [C.POINTER(Data), C.c_longlong, dp, C.c_double, dp, C.c_int]
     L.gdn_cuda_instance_info.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                          C.POINTER(C.c_longlong)]
     _lib = L
@@ -253,6 +256,22 @@ def cavity_data():
     return d
 
 
+def stationary_data():
+    """maxwell_imposed_stationary (src/models/maxwell.c:16-84)."""
+    d = cavity_data()
+    d.kind = DATA_STATIONARY
+    return d
+
+
+def eval_data(data: Data, xyz: np.ndarray, t: float, device: int = 0) -> np.ndarray:
+    """The analytic data at points xyz[n, 3] and time t, evaluated on the
+    device by the solver's own code: [n, 6]."""
+    x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    w = np.zeros((len(x), 6))
+    check(lib().gdn_cuda_eval_data(C.byref(data), len(x), _dp(x), float(t), _dp(w), device))
+    return w
+
+
 class Solver:
     """One attach handle (the device-side replacement of a gdn_simulation's
     assembled operators)."""
@@ -322,6 +341,10 @@ class Solver:
     def save_xdmf(self, basename: str, iter_id: int, instance: int = 0):
         """io_save_all of the current state (raw binary + XDMF files)."""
         check(self.L.gdn_cuda_save_xdmf(self.h, int(instance), basename.encode(), int(iter_id)))
+
+    def set_wait_limit(self, polls: int):
+        """Polls after which a bounded device-side wait gives up (test hook)."""
+        check(self.L.gdn_cuda_set_wait_limit(self.h, int(polls)))
 
     def error_l2(self) -> float:
         e = C.c_double()

@@ -112,9 +112,15 @@ struct gdn_cuda_handle {
 	double *yacc = nullptr; // FP32_REFINE: FP64 solution of the transport solve
 	float *rhs = nullptr; // FP32_REFINE: residual, right-hand side of the corrections
 	int refine_passes = 1;
-	int kin_mode = 1; // 1: a launch per sweep level, 2: one cooperative launch per sweep
-	bool kin_autotune = true; // pick kin_mode at attach by timing both
+	int kin_mode = 1; // 1: a launch per sweep level, 2: one cooperative launch per sweep, 3: flag-driven
+	bool kin_autotune = true; // pick kin_mode at attach by timing the modes
 	int kin_grid[3] = {0, 0, 0}; // CTAs of the cooperative sweep, per accumulate mode
+	int kin_fgrid[3] = {0, 0, 0}; // CTAs of the flag-driven sweep, per accumulate mode
+	int2 *kchunks = nullptr; // [nchunks] level-aligned 32-item chunks (first item, end item)
+	int nchunks = 0;
+	int *kready = nullptr; // [nitems] readiness flags of the flag-driven sweep
+	unsigned *kqueue = nullptr; // its chunk counter
+	long long spin_limit = 1LL << 21; // polls of a bounded device-side wait (~1 s)
 	int max_chunks = 1; // most 32-item chunks in one level
 	int *level_off_dev = nullptr;
 	unsigned *bar = nullptr; // [2] grid barrier of the cooperative sweep
@@ -291,7 +297,8 @@ static int validate_mesh(const gdn_cuda_mesh *m)
 
 static int validate_data(const gdn_cuda_data *d)
 {
-	if (!d || (d->kind != GDN_CUDA_DATA_PLANE && d->kind != GDN_CUDA_DATA_CAVITY))
+	if (!d || (d->kind != GDN_CUDA_DATA_PLANE && d->kind != GDN_CUDA_DATA_CAVITY &&
+			   d->kind != GDN_CUDA_DATA_STATIONARY))
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown analytic data kind");
 	if (d->kind == GDN_CUDA_DATA_PLANE) {
 		const double kk = d->khat[0] * d->khat[0] + d->khat[1] * d->khat[1] + d->khat[2] * d->khat[2];
@@ -642,10 +649,20 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		GDN_TRY(dalloc(h, &h->err, 1));
 		GDN_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned), s));
 		GDN_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
+		// the flag-driven sweep: level-aligned chunks in sweep order
+		std::vector<int2> chunks;
 		for (int l = 0; l < nl; l++) {
 			const int nch = (h->level_off[l + 1] - h->level_off[l] + 31) / 32;
 			h->max_chunks = nch > h->max_chunks ? nch : h->max_chunks;
+			for (int k0 = h->level_off[l]; k0 < h->level_off[l + 1]; k0 += 32)
+				chunks.push_back(make_int2(k0, k0 + 32 < h->level_off[l + 1] ? k0 + 32 : h->level_off[l + 1]));
 		}
+		h->nchunks = (int)chunks.size();
+		GDN_TRY(dalloc(h, &h->kchunks, chunks.size()));
+		GDN_CUDA_TRY(cudaMemcpyAsync(h->kchunks, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice,
+									 s));
+		GDN_TRY(dalloc(h, &h->kready, nu));
+		GDN_TRY(dalloc(h, &h->kqueue, 1));
 		GDN_TRY(kin_prepare_grids(h));
 		GDN_CUDA_TRY(cudaStreamSynchronize(s));
 		if (h->kin_autotune)
@@ -792,8 +809,8 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
 	if (cfg.rk3_variant < 0 || cfg.rk3_variant > 2)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: rk3_variant must be 0 (auto), 1 or 2");
-	if (cfg.kin_sweep < 0 || cfg.kin_sweep > 2)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kin_sweep must be 0 (auto), 1 or 2");
+	if (cfg.kin_sweep < 0 || cfg.kin_sweep > 3)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kin_sweep must be 0 (auto), 1, 2 or 3");
 	for (int i = 0; i < n; i++) {
 		GDN_TRY(validate_mesh(inst[i].mesh));
 		GDN_TRY(validate_data(inst[i].data));
@@ -823,7 +840,7 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 	// SM; 0 = timed at attach
 	h->rk3_variant = cfg.rk3_variant > 0 ? cfg.rk3_variant - 1 : 0;
 	h->rk3_autotune = cfg.rk3_variant == 0;
-	h->kin_mode = cfg.kin_sweep == 2 ? 2 : 1;
+	h->kin_mode = cfg.kin_sweep == 0 ? 1 : cfg.kin_sweep;
 	h->kin_autotune = cfg.kin_sweep == 0;
 	h->ninst = n;
 	for (int i = 0; i < n; i++) {
@@ -971,8 +988,17 @@ static int kin_sweeps(gdn_cuda_handle *h, const void *f, int acc, int bdata, lon
 		grid = grid > 0 ? grid : 1;
 		p.item_begin = 0;
 		p.item_end = h->level_off[nl];
-		GDN_TRY((launch_kin_levels<F, Y, T>(p, h->level_off_dev, nl, grid, h->bar, h->err, acc, bdata, h->rk3_sparse,
-											h->stream)));
+		GDN_TRY((launch_kin_levels<F, Y, T>(p, h->level_off_dev, nl, grid, h->bar, h->err, h->spin_limit, acc, bdata,
+											h->rk3_sparse, h->stream)));
+		nlaunch++;
+		return GDN_CUDA_OK;
+	}
+	if (h->kin_mode == 3) {
+		p.item_begin = 0;
+		p.item_end = h->level_off[nl];
+		GDN_TRY((launch_kin_flags<F, Y, T>(p, h->kchunks, h->nchunks, h->kin_fgrid[acc] > 0 ? h->kin_fgrid[acc] : 1,
+										   h->kqueue, h->kready, h->ne * h->nv, h->err, h->spin_limit, acc, bdata,
+										   h->rk3_sparse, h->stream)));
 		nlaunch++;
 		return GDN_CUDA_OK;
 	}
@@ -1055,10 +1081,28 @@ static int kin_enqueue(gdn_cuda_handle *h, long long &nlaunch)
 	return GDN_CUDA_OK;
 }
 
-// CTAs of the cooperative sweep for the variants this handle's precision runs
+// CTAs of the cooperative and the flag-driven sweeps for the variants this
+// handle's precision runs
+static int kin_prepare_flag_grids(gdn_cuda_handle *h)
+{
+	const int sp = h->rk3_sparse;
+	switch (h->precision) {
+	case GDN_CUDA_FP64:
+		return kin_flags_grid<double, double, double>(h->device, 0, sp, &h->kin_fgrid[0]);
+	case GDN_CUDA_FP32:
+		return kin_flags_grid<float, float, float>(h->device, 0, sp, &h->kin_fgrid[0]);
+	case GDN_CUDA_BF16_STORE:
+		return kin_flags_grid<__nv_bfloat16, float, float>(h->device, 0, sp, &h->kin_fgrid[0]);
+	default:
+		GDN_TRY((kin_flags_grid<double, float, float>(h->device, 1, sp, &h->kin_fgrid[1])));
+		return kin_flags_grid<float, float, float>(h->device, 2, sp, &h->kin_fgrid[2]);
+	}
+}
+
 static int kin_prepare_grids(gdn_cuda_handle *h)
 {
 	const int sp = h->rk3_sparse;
+	GDN_TRY(kin_prepare_flag_grids(h));
 	switch (h->precision) {
 	case GDN_CUDA_FP64:
 		return kin_levels_grid<double, double, double>(h->device, 0, sp, &h->kin_grid[0]);
@@ -1119,7 +1163,7 @@ static int autotune_kin(gdn_cuda_handle *h)
 	GDN_CUDA_TRY(cudaEventCreate(&ev[1]));
 	float best = 0.f;
 	int pick = 1, rc = GDN_CUDA_OK;
-	for (int mode = 1; mode <= 2 && rc == GDN_CUDA_OK; mode++) {
+	for (int mode = 1; mode <= 3 && rc == GDN_CUDA_OK; mode++) {
 		h->kin_mode = mode;
 		long long nlaunch = 0;
 		rc = kin_first_sweep(h, nlaunch); // warm-up
@@ -1725,6 +1769,59 @@ extern "C" int gdn_cuda_space_convergence(const gdn_cuda_mesh *const *meshes, in
 		order_out[k] = k == 0 ? -1.0 : conv_order(err_out[k - 1], err_out[k], hmin_out[k - 1], hmin_out[k]);
 	}
 	return GDN_CUDA_OK;
+}
+
+extern "C" int gdn_cuda_set_wait_limit(gdn_cuda_handle *h, long long polls)
+{
+	if (!h || polls < 0)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "set_wait_limit: bad arguments");
+	GDN_CUDA_TRY(cudaSetDevice(h->device));
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	h->spin_limit = polls;
+	// the limit is a kernel parameter of the captured step loops
+	for (int k = 0; k < 2; k++)
+		if (h->graph_exec[k]) {
+			cudaGraphExecDestroy(h->graph_exec[k]);
+			h->graph_exec[k] = nullptr;
+		}
+	return GDN_CUDA_OK;
+}
+
+// ------------------------------------------------------ data check --
+extern "C" int gdn_cuda_eval_data(const gdn_cuda_data *d, long long npts, const double *xyz, double t, double *w,
+								  int device)
+{
+	if (!d || npts < 0 || (npts > 0 && (!xyz || !w)))
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "eval_data: bad arguments");
+	GDN_TRY(validate_data(d));
+	if (npts == 0)
+		return GDN_CUDA_OK;
+	GDN_CUDA_TRY(cudaSetDevice(device));
+	cudaStream_t s = nullptr;
+	double *xd = nullptr, *wd = nullptr;
+	int rc = GDN_CUDA_OK;
+	cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+	if (e == cudaSuccess)
+		e = cudaMalloc(&xd, (size_t)npts * 3 * sizeof(double));
+	if (e == cudaSuccess)
+		e = cudaMalloc(&wd, (size_t)npts * 6 * sizeof(double));
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(xd, xyz, (size_t)npts * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
+	if (e == cudaSuccess) {
+		rc = launch_eval_data(xd, npts, to_data(d), t, wd, s);
+		if (rc == GDN_CUDA_OK)
+			e = cudaMemcpyAsync(w, wd, (size_t)npts * 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
+	}
+	if (e == cudaSuccess && rc == GDN_CUDA_OK)
+		e = cudaStreamSynchronize(s);
+	if (e != cudaSuccess && rc == GDN_CUDA_OK)
+		rc = e == cudaErrorMemoryAllocation ? gdn_set_error(GDN_CUDA_ERR_OOM, "eval_data: device allocation failed")
+											: gdn_cuda_fail(e, "eval_data", __FILE__, __LINE__);
+	cudaFree(xd);
+	cudaFree(wd);
+	if (s)
+		cudaStreamDestroy(s);
+	return rc;
 }
 
 extern "C" int gdn_cuda_get_time(gdn_cuda_handle *h, double *t)

@@ -252,6 +252,28 @@ int launch_boundary_dofs(const double *bxyz, long long nbf, const Data &d, doubl
 	return GDN_CUDA_OK;
 }
 
+// the analytic data at arbitrary points: w[i][c] = w_exact(xyz[i], t)_c
+__global__ void eval_data_kernel(const double *__restrict__ xyz, long long n, Data d, double t,
+								 double *__restrict__ w)
+{
+	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (u >= n)
+		return;
+	double x[3] = {xyz[3 * u], xyz[3 * u + 1], xyz[3 * u + 2]}, we[6];
+	exact_w(d, x, t, we);
+	for (int c = 0; c < 6; c++)
+		w[u * 6 + c] = we[c];
+}
+
+int launch_eval_data(const double *xyz, long long n, const Data &d, double t, double *w, cudaStream_t s)
+{
+	if (n <= 0)
+		return GDN_CUDA_OK;
+	eval_data_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(xyz, n, d, t, w);
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+
 // kinetic device layout f[k][c][i], k = pos[e * nv + v]
 //   <->  wn[(c*nv + v)*neq + 10 e + i]
 template <typename S>

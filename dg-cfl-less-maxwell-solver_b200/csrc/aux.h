@@ -24,6 +24,7 @@ int launch_init_kin(const int *e2q, const double *node, long long ne, const Data
 					const int *pos, S *f, cudaStream_t s);
 int launch_boundary_dofs(const double *bxyz, long long nbf, const Data &d, double t, int kinetic,
 						 const KinModel &km, long long neq, double *out, cudaStream_t s);
+int launch_eval_data(const double *xyz, long long n, const Data &d, double t, double *w, cudaStream_t s);
 template <typename S>
 int launch_kin_pack(const S *f, const int *pos, long long ne, int nv, long long neq, double *wn, int to_ref,
 					cudaStream_t s);

@@ -96,9 +96,47 @@ struct Data {
 	double phase;
 };
 
+// The stationary data maxwell_imposed_stationary (src/models/maxwell.c:16-84):
+// E = (g(x0) + f(x1, x2), g(x1) + f(x2, x0), g(x2) + f(x0, x1)) constant in
+// time, H growing linearly in t from the derivatives of f.  Products are
+// formed in the reference's left-to-right order; g and f use the full pi,
+// the derivative terms its 10-digit pi 3.141592654.
+namespace stationary {
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kPi10 = 0.3141592654e1;
+__device__ __forceinline__ double g(double x)
+{
+	return sin(2.0 * kPi * (x - 0.5));
+}
+__device__ __forceinline__ double f(double y, double z)
+{
+	return exp(-2.0 * kPi * (y - 0.5)) * sin(2.0 * kPi * (z - 0.5)) +
+		   exp(-2.0 * kPi * (z - 0.5)) * sin(2.0 * kPi * (y - 0.5));
+}
+// d f / d(first argument), d f / d(second argument)
+__device__ __forceinline__ double df1(double y, double z)
+{
+	return -2.0 * kPi10 * exp(-2.0 * kPi10 * (y - 0.5)) * sin(2.0 * kPi10 * (z - 0.5)) +
+		   2.0 * exp(-2.0 * kPi10 * (z - 0.5)) * kPi10 * cos(2.0 * kPi10 * (y - 0.5));
+}
+__device__ __forceinline__ double df2(double y, double z)
+{
+	return 2.0 * exp(-2.0 * kPi10 * (y - 0.5)) * kPi10 * cos(2.0 * kPi10 * (z - 0.5)) -
+		   2.0 * exp(-2.0 * kPi10 * (z - 0.5)) * kPi10 * sin(2.0 * kPi10 * (y - 0.5));
+}
+} // namespace stationary
+
 __device__ __forceinline__ void exact_w(const Data &d, const double x[3], double t, double w[6])
 {
-	if (d.kind == GDN_CUDA_DATA_CAVITY) {
+	if (d.kind == GDN_CUDA_DATA_STATIONARY) {
+		// the reference's damping factor exp(-sigma t) has sigma = 0: a factor 1
+		w[0] = stationary::g(x[0]) + stationary::f(x[1], x[2]);
+		w[1] = stationary::g(x[1]) + stationary::f(x[2], x[0]);
+		w[2] = stationary::g(x[2]) + stationary::f(x[0], x[1]);
+		w[3] = (stationary::df1(x[2], x[0]) - stationary::df2(x[0], x[1])) * t;
+		w[4] = (stationary::df1(x[0], x[1]) - stationary::df2(x[1], x[2])) * t;
+		w[5] = (stationary::df1(x[1], x[2]) - stationary::df2(x[2], x[0])) * t;
+	} else if (d.kind == GDN_CUDA_DATA_CAVITY) {
 		// maxwell_imposed_macro_cavity (src/models/maxwell.c:118-133), with
 		// its truncated pi 3.141592654
 		const double pi = 0.3141592654e1;

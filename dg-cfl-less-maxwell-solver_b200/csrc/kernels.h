@@ -100,9 +100,20 @@ int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cu
 // barrier that times out sets *err.
 template <typename F, typename Y, typename T>
 int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels, int grid, unsigned *bar, int *err,
-					  int acc, int bdata, int sparse, cudaStream_t s);
+					  long long spin_limit, int acc, int bdata, int sparse, cudaStream_t s);
 template <typename F, typename Y, typename T>
 int kin_levels_grid(int device, int acc, int sparse, int *grid);
+
+// The same solve driven by per-item readiness flags in one launch: CTAs take
+// level-aligned 32-item chunks (chunks[c] = first item, end item) in sweep
+// order from *queue and wait only for their items' upwind neighbours' flags
+// (ready[nitems], cleared with *queue before the launch); a wait that gives
+// up after spin_limit polls sets *err.
+template <typename F, typename Y, typename T>
+int launch_kin_flags(const KinSweepParams &p, const int2 *chunks, int nchunks, int grid, unsigned *queue, int *ready,
+					 long long nitems, int *err, long long spin_limit, int acc, int bdata, int sparse, cudaStream_t s);
+template <typename F, typename Y, typename T>
+int kin_flags_grid(int device, int acc, int sparse, int *grid);
 
 // Level schedule of the upwind item graph on the device: items[k] (e * nv +
 // v in level order, ascending within a level), pos (its inverse), level_off

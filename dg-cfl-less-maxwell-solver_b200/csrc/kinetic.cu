@@ -208,90 +208,146 @@ int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, 
 	return rc;
 }
 
-// G = D^-1 per (element, velocity), FP64 Gauss-Jordan with partial
-// pivoting, written at the item's sweep position with theta dt / det.
+// G = D^-1 per (element, velocity), FP64 Gauss-Jordan with partial pivoting
+// on [D | I], written at the item's sweep position with theta dt / det.
+// Sixteen lanes per item, lane r < 10 holding row r of [D | I] in registers
+// (no local memory): the pivot of column k is found by a shuffle reduction
+// over the rows not yet used, the pivot row is broadcast by shuffles, and
+// every other row eliminates column k.  Rows are not moved: each lane keeps
+// the position its row would have in the row-swapping algorithm, so that the
+// pivot choice (largest |a|, ties to the smallest position) and every
+// arithmetic operation are those of the textbook in-place version.  Columns
+// left of the pivot are not updated: they no longer feed a pivot or the
+// inverse.
+constexpr int kBlkThreads = 256; // 16 items per CTA
 template <typename GT>
-__global__ void kin_blocks_kernel(const double *__restrict__ geom, const double *__restrict__ sown64,
-								  const int *__restrict__ pos, long long ne, KinModel km, double theta,
-								  const int *__restrict__ einst, const double *__restrict__ dt_tab,
-								  GT *__restrict__ G, GT *__restrict__ rcoef, double4 *__restrict__ ru64,
-								  double4 *__restrict__ rs64, int *__restrict__ bad)
+__global__ void __launch_bounds__(kBlkThreads)
+	kin_blocks_kernel(const double *__restrict__ geom, const double *__restrict__ sown64,
+					  const int *__restrict__ pos, long long ne, KinModel km, double theta,
+					  const int *__restrict__ einst, const double *__restrict__ dt_tab, GT *__restrict__ G,
+					  GT *__restrict__ rcoef, double4 *__restrict__ ru64, double4 *__restrict__ rs64,
+					  int *__restrict__ bad)
 {
-	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (u >= ne * km.nv)
-		return;
+	__shared__ double sMinv[10][10];
+	const Tables<double> &tb = c_tab_d;
+	for (int q = threadIdx.x; q < 100; q += blockDim.x)
+		sMinv[q / 10][q % 10] = tb.Minv[q / 10][q % 10];
+	__syncthreads();
+	const int lane = threadIdx.x & 31, r = lane & 15;
+	const long long nu = ne * km.nv;
+	const long long u0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4;
+	const bool item = u0 < nu;
+	const long long u = item ? u0 : nu - 1; // lanes past the end shadow the last item
+	const bool row = r < 10;
+	const int rr = row ? r : 0;
 	const long long e = u / km.nv;
 	const int v = (int)(u % km.nv);
-	const Tables<double> &tb = c_tab_d;
 	const double *vv = km.vi + 3 * v;
 	double cod[3][3];
+#pragma unroll
 	for (int a = 0; a < 3; a++)
+#pragma unroll
 		for (int b = 0; b < 3; b++)
 			cod[a][b] = geom[e * 10 + 3 * a + b];
 	const double det = geom[e * 10 + 9];
 	// u_k = sum_l v_l codtau[l][k]:  v . c_ij = sum_k u_k int d_k phi_i phi_j
 	double uk[3];
+#pragma unroll
 	for (int k = 0; k < 3; k++)
 		uk[k] = vv[0] * cod[0][k] + vv[1] * cod[1][k] + vv[2] * cod[2][k];
-	double F[10][10];
-	for (int i = 0; i < 10; i++)
-		for (int j = 0; j < 10; j++)
-			F[i][j] = -(uk[0] * tb.D[0][i][j] + uk[1] * tb.D[1][i][j] + uk[2] * tb.D[2][i][j]);
+	double sp[4];
+#pragma unroll
 	for (int f = 0; f < 4; f++) {
-		const double s = sown64[u * 4 + f];
-		const double sp = s > 0.0 ? s : 0.0;
-		if (sp == 0.0)
-			continue;
-		for (int ii = 0; ii < 6; ii++)
-			for (int jj = 0; jj < 6; jj++)
-				F[tb.f2n[f][ii]][tb.f2n[f][jj]] += sp * tb.S[ii][jj];
+		const double sf = sown64[u * 4 + f];
+		sp[f] = sf > 0.0 ? sf : 0.0;
 	}
 	const double c = theta * dt_tab[einst ? einst[e] : 0] / det;
-	double a[10][20];
-	for (int i = 0; i < 10; i++) {
-		for (int j = 0; j < 10; j++) {
-			double acc = 0.0;
-			for (int k = 0; k < 10; k++)
-				acc += tb.Minv[i][k] * F[k][j];
-			a[i][j] = (i == j ? 1.0 : 0.0) + c * acc;
-			a[i][10 + j] = i == j ? 1.0 : 0.0;
+	// row rr of [I + c Minv F | I], F = V + sum_outflow s+ E S E^T, column by
+	// column of F
+	double a[20];
+#pragma unroll
+	for (int j = 0; j < 10; j++) {
+		double F[10];
+#pragma unroll
+		for (int i = 0; i < 10; i++)
+			F[i] = -(uk[0] * tb.D[0][i][j] + uk[1] * tb.D[1][i][j] + uk[2] * tb.D[2][i][j]);
+#pragma unroll
+		for (int f = 0; f < 4; f++) {
+			if (sp[f] == 0.0)
+				continue;
+#pragma unroll
+			for (int jj = 0; jj < 6; jj++)
+				if (f2n(f, jj) == j)
+#pragma unroll
+					for (int ii = 0; ii < 6; ii++)
+						F[f2n(f, ii)] += sp[f] * tb.S[ii][jj];
 		}
+		double acc = 0.0;
+#pragma unroll
+		for (int k = 0; k < 10; k++)
+			acc += sMinv[rr][k] * F[k];
+		a[j] = (rr == j ? 1.0 : 0.0) + c * acc;
+		a[10 + j] = rr == j ? 1.0 : 0.0;
 	}
+	int posn = rr; // this row's position in the row-swapping algorithm
+	bool singular = false;
+#pragma unroll
 	for (int k = 0; k < 10; k++) {
-		int piv = k;
-		for (int r = k + 1; r < 10; r++)
-			if (fabs(a[r][k]) > fabs(a[piv][k]))
-				piv = r;
-		if (piv != k)
-			for (int q = 0; q < 20; q++) {
-				double t = a[k][q];
-				a[k][q] = a[piv][q];
-				a[piv][q] = t;
+		// pivot: the largest |a[k]| among positions >= k, ties to the smallest position
+		double best = row && posn >= k ? fabs(a[k]) : -1.0;
+		int bpos = row ? posn : 99, blane = lane;
+#pragma unroll
+		for (int off = 8; off > 0; off >>= 1) {
+			const double ob = __shfl_xor_sync(0xffffffffu, best, off, 16);
+			const int op = __shfl_xor_sync(0xffffffffu, bpos, off, 16);
+			const int ol = __shfl_xor_sync(0xffffffffu, blane, off, 16);
+			if (ob > best || (ob == best && op < bpos)) {
+				best = ob;
+				bpos = op;
+				blane = ol;
 			}
-		if (a[k][k] == 0.0) {
-			atomicMax(bad, 1);
-			return;
 		}
-		const double inv = 1.0 / a[k][k];
-		for (int q = 0; q < 20; q++)
-			a[k][q] *= inv;
-		for (int r = 0; r < 10; r++)
-			if (r != k) {
-				const double m = a[r][k];
-				if (m != 0.0)
-					for (int q = 0; q < 20; q++)
-						a[r][q] -= m * a[k][q];
+		// the rows at position k and at the pivot's position trade places
+		if (row && posn == k)
+			posn = bpos;
+		else if (lane == blane)
+			posn = k;
+		if (lane == blane) {
+			if (a[k] == 0.0) {
+				singular = true;
+			} else {
+				const double inv = 1.0 / a[k];
+#pragma unroll
+				for (int q = k; q < 20; q++)
+					a[q] *= inv;
 			}
+		}
+		singular = __shfl_sync(0xffffffffu, (int)singular, blane, 16) != 0 || singular;
+		const double m = a[k];
+#pragma unroll
+		for (int q = k; q < 20; q++) {
+			const double pq = __shfl_sync(0xffffffffu, a[q], blane, 16);
+			if (row && lane != blane && m != 0.0)
+				a[q] -= m * pq;
+		}
 	}
-	const long long k = pos[u];
-	GT *Gk = G + k * 100;
-	for (int i = 0; i < 10; i++)
-		for (int j = 0; j < 10; j++)
-			Gk[i * 10 + j] = (GT)a[i][10 + j];
-	rcoef[k] = (GT)c;
-	if (ru64) {
-		ru64[k] = make_double4(uk[0], uk[1], uk[2], c);
-		rs64[k] = make_double4(sown64[u * 4], sown64[u * 4 + 1], sown64[u * 4 + 2], sown64[u * 4 + 3]);
+	if (!item || !row)
+		return;
+	if (singular) {
+		atomicMax(bad, 1);
+		return;
+	}
+	const long long kk = pos[u];
+	GT *Gk = G + kk * 100 + posn * 10;
+#pragma unroll
+	for (int j = 0; j < 10; j++)
+		Gk[j] = (GT)a[10 + j];
+	if (r == 0) {
+		rcoef[kk] = (GT)c;
+		if (ru64) {
+			ru64[kk] = make_double4(uk[0], uk[1], uk[2], c);
+			rs64[kk] = make_double4(sown64[u * 4], sown64[u * 4 + 1], sown64[u * 4 + 2], sown64[u * 4 + 3]);
+		}
 	}
 }
 
@@ -344,8 +400,8 @@ int launch_kin_blocks(const double *geom, const double *sown64, const int *items
 					  double4 *rs64, int *bad, cudaStream_t s)
 {
 	const long long nu = ne * km.nv;
-	kin_blocks_kernel<GT><<<(unsigned)((nu + 127) / 128), 128, 0, s>>>(geom, sown64, pos, ne, km, theta, einst,
-																	   dt_tab, G, rcoef, ru64, rs64, bad);
+	kin_blocks_kernel<GT><<<(unsigned)((nu * 16 + kBlkThreads - 1) / kBlkThreads), kBlkThreads, 0, s>>>(
+		geom, sown64, pos, ne, km, theta, einst, dt_tab, G, rcoef, ru64, rs64, bad);
 	GDN_CUDA_TRY(cudaGetLastError());
 	kin_records_kernel<GT><<<(unsigned)((nu + 255) / 256), 256, 0, s>>>(items, pos, sown64, nb, perm, nu, km.nv, rnb,
 																		rpm, rs);
@@ -477,11 +533,14 @@ struct SweepG {
 };
 
 // 32 consecutive items [k0, min(k0 + 32, item_end)) of one level.  `wait` is
-// called after the prologue (records, right-hand side, G staging: data no
-// sweep level writes) and before the first trace load.  L2 = true reads the
-// traces through L2 only (L1 is not coherent with other SMs' writes made
-// during the same launch).
-template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE, bool L2, typename Wait>
+// called by every thread after the prologue (records, right-hand side, G
+// staging: data no sweep level writes) and before its first trace load, with
+// its item's inflow records nbk[4] (item index >= 0 for an upwind neighbour)
+// and whether the thread holds an item.  L2 = true reads the traces through
+// L2 only (L1 is not coherent with other SMs' writes made during the same
+// launch); FENCE = true orders every thread's y stores device-wide before the
+// chunk's closing barrier, so that one thread can then publish them.
+template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE, bool L2, bool FENCE, typename Wait>
 __device__ __forceinline__ void sweep_chunk(const KinSweepParams &p, long long k0, long long item_end, T *gsh,
 											Wait wait)
 {
@@ -522,7 +581,7 @@ __device__ __forceinline__ void sweep_chunk(const KinSweepParams &p, long long k
 	int v = 0;
 	if (BD)
 		v = p.items[k] % p.nv;
-	wait();
+	wait(nbk, act);
 	T r[10];
 	{
 		T tr[4][6];
@@ -601,6 +660,8 @@ __device__ __forceinline__ void sweep_chunk(const KinSweepParams &p, long long k
 			store10<double, double>(p.yacc + k * 60 + c * 10, ya);
 		}
 	}
+	if (FENCE)
+		__threadfence();
 	// gsh is reused by the CTA's next chunk
 	__syncthreads();
 }
@@ -616,8 +677,8 @@ __global__ void __launch_bounds__(kSwThreads) kin_sweep_kernel(KinSweepParams p)
 	const long long k0 = (long long)p.item_begin + (long long)blockIdx.x * kSwItems;
 	// the upwind items of earlier levels are complete once the previous
 	// level's grid is
-	sweep_chunk<F, Y, T, ACC, BD, SPARSE, false>(p, k0, p.item_end, gsh,
-												[] { asm volatile("griddepcontrol.wait;" ::: "memory"); });
+	sweep_chunk<F, Y, T, ACC, BD, SPARSE, false, false>(
+		p, k0, p.item_end, gsh, [](const int *, bool) { asm volatile("griddepcontrol.wait;" ::: "memory"); });
 }
 
 // Grid-wide barrier of a cooperative launch (all CTAs co-resident).  *count
@@ -670,7 +731,7 @@ __global__ void __launch_bounds__(kSwThreads) kin_levels_kernel(KinSweepParams p
 		bool ok = true;
 		const unsigned target = (unsigned)l * gridDim.x;
 		for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-			sweep_chunk<F, Y, T, ACC, BD, SPARSE, true>(p, b + ch * kSwItems, e, gsh, [&] {
+			sweep_chunk<F, Y, T, ACC, BD, SPARSE, true, false>(p, b + ch * kSwItems, e, gsh, [&](const int *, bool) {
 				if (pending) {
 					ok = grid_barrier(bar, target, err, spin_limit);
 					pending = false;
@@ -681,6 +742,75 @@ __global__ void __launch_bounds__(kSwThreads) kin_levels_kernel(KinSweepParams p
 		}
 		if (pending && !grid_barrier(bar, target, err, spin_limit))
 			return;
+	}
+}
+
+// Bounded wait for an upwind item's readiness flag (acquire): true once it is
+// set; false when *err is set by another CTA, or after spin_limit further
+// polls (then *err is set here), so a lost producer ends the launch instead
+// of hanging it.
+__device__ __forceinline__ bool wait_ready(const int *flag, int *err, long long spin_limit)
+{
+	int v;
+	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+	if (v)
+		return true;
+	const volatile int *verr = err;
+	for (long long it = 0; it < spin_limit; it++) {
+		if (*verr)
+			return false;
+		__nanosleep(20);
+		asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+		if (v)
+			return true;
+	}
+	atomicExch(err, 1);
+	return false;
+}
+
+// The whole transport solve in one launch, driven by per-item readiness flags
+// instead of a barrier per level.  chunks[] lists the solve's 32-item chunks
+// in sweep order, never straddling a level, so every upwind item of a chunk
+// lies in an earlier chunk.  Each CTA takes the next chunk from an atomic
+// counter, stages it, waits (acquire) only for the flags of its own items'
+// upwind neighbours, solves, and publishes its items' flags (release).  A
+// chunk waits only on chunks taken earlier by CTAs already running, so the
+// solve progresses with any number of resident CTAs; the critical path is the
+// longest upwind chain, not the level count times a launch.  ready[] (one int
+// per item) and *queue are zero at launch.
+template <typename F, typename Y, typename T, int ACC, bool BD, bool SPARSE>
+__global__ void __launch_bounds__(kSwThreads)
+	kin_flags_kernel(KinSweepParams p, const int2 *__restrict__ chunks, int nchunks, unsigned *queue, int *ready,
+					 int *err, long long spin_limit)
+{
+	__shared__ __align__(16) T gsh[kSwItems * SweepG<T>::stride];
+	__shared__ int s_chunk, s_fail;
+	for (;;) {
+		__syncthreads(); // the previous chunk's s_chunk / s_fail have been read
+		if (threadIdx.x == 0) {
+			s_chunk = (int)atomicAdd(queue, 1u);
+			s_fail = 0;
+		}
+		__syncthreads();
+		const int c = s_chunk;
+		if (c >= nchunks)
+			return;
+		const int2 ck = chunks[c];
+		sweep_chunk<F, Y, T, ACC, BD, SPARSE, true, true>(
+			p, ck.x, ck.y, gsh, [&](const int *nbk, bool act) {
+				if (!act)
+					return;
+#pragma unroll
+				for (int f = 0; f < 4; f++)
+					if (nbk[f] >= 0 && !wait_ready(ready + nbk[f], err, spin_limit))
+						s_fail = 1;
+			});
+		// sweep_chunk ended with a barrier after every thread's fenced y stores
+		if (s_fail)
+			return; // *err is set; the state of this solve is invalid
+		if (threadIdx.x < ck.y - ck.x)
+			asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(ready + ck.x + threadIdx.x), "r"(1)
+						 : "memory");
 	}
 }
 
@@ -725,7 +855,7 @@ int launch_kin_sweep(const KinSweepParams &p, int acc, int bdata, int sparse, cu
 }
 template <typename F, typename Y, typename T>
 int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels, int grid, unsigned *bar, int *err,
-					  int acc, int bdata, int sparse, cudaStream_t s)
+					  long long spin, int acc, int bdata, int sparse, cudaStream_t s)
 {
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3((unsigned)grid);
@@ -737,7 +867,6 @@ int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels
 	attr[0].val.cooperative = 1;
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
-	const long long spin = 1LL << 21; // each poll is an L2 round trip: a lost CTA ends the launch in ~1 s
 	GDN_CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(unsigned), s));
 #define GDN_LEVELS(A, B, SP)                                                                                          \
 	GDN_CUDA_TRY(cudaLaunchKernelEx(&cfg, kin_levels_kernel<F, Y, T, A, B, SP>, p, level_off, nlevels, bar, err, spin))
@@ -764,6 +893,60 @@ int launch_kin_levels(const KinSweepParams &p, const int *level_off, int nlevels
 	return GDN_CUDA_OK;
 }
 
+template <typename F, typename Y, typename T>
+int launch_kin_flags(const KinSweepParams &p, const int2 *chunks, int nchunks, int grid, unsigned *queue, int *ready,
+					 long long nitems, int *err, long long spin, int acc, int bdata, int sparse, cudaStream_t s)
+{
+	if (nchunks <= 0)
+		return GDN_CUDA_OK;
+	GDN_CUDA_TRY(cudaMemsetAsync(ready, 0, (size_t)nitems * sizeof(int), s));
+	GDN_CUDA_TRY(cudaMemsetAsync(queue, 0, sizeof(unsigned), s));
+	const unsigned g = (unsigned)(grid < nchunks ? grid : nchunks);
+#define GDN_FLAGS(A, B, SP)                                                                                           \
+	kin_flags_kernel<F, Y, T, A, B, SP><<<g, kSwThreads, 0, s>>>(p, chunks, nchunks, queue, ready, err, spin)
+	if (acc == 0 && bdata) {
+		if (sparse)
+			GDN_FLAGS(0, true, true);
+		else
+			GDN_FLAGS(0, true, false);
+	} else if (acc == 1 && bdata) {
+		if (sparse)
+			GDN_FLAGS(1, true, true);
+		else
+			GDN_FLAGS(1, true, false);
+	} else if (acc == 2 && !bdata) {
+		if (sparse)
+			GDN_FLAGS(2, false, true);
+		else
+			GDN_FLAGS(2, false, false);
+	} else {
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "kinetic sweep: unsupported accumulate / boundary mode");
+	}
+#undef GDN_FLAGS
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
+}
+
+// CTAs of the flag-driven sweep that fit on the device at once
+template <typename F, typename Y, typename T>
+int kin_flags_grid(int device, int acc, int sparse, int *grid)
+{
+	int nsm = 0, per = 0;
+	GDN_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+	const void *fn;
+	if (sparse)
+		fn = acc == 0   ? (const void *)kin_flags_kernel<F, Y, T, 0, true, true>
+			 : acc == 1 ? (const void *)kin_flags_kernel<F, Y, T, 1, true, true>
+						: (const void *)kin_flags_kernel<F, Y, T, 2, false, true>;
+	else
+		fn = acc == 0   ? (const void *)kin_flags_kernel<F, Y, T, 0, true, false>
+			 : acc == 1 ? (const void *)kin_flags_kernel<F, Y, T, 1, true, false>
+						: (const void *)kin_flags_kernel<F, Y, T, 2, false, false>;
+	GDN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kSwThreads, 0));
+	*grid = nsm * (per > 0 ? per : 1);
+	return GDN_CUDA_OK;
+}
+
 // CTAs of the persistent level loop that fit on the device at once
 template <typename F, typename Y, typename T>
 int kin_levels_grid(int device, int acc, int sparse, int *grid)
@@ -785,9 +968,12 @@ int kin_levels_grid(int device, int acc, int sparse, int *grid)
 }
 
 #define GDN_LEVELS_INST(F, Y, T)                                                                                      \
-	template int launch_kin_levels<F, Y, T>(const KinSweepParams &, const int *, int, int, unsigned *, int *, int, int,  \
-											int, cudaStream_t);                                                          \
-	template int kin_levels_grid<F, Y, T>(int, int, int, int *);
+	template int launch_kin_levels<F, Y, T>(const KinSweepParams &, const int *, int, int, unsigned *, int *,         \
+											long long, int, int, int, cudaStream_t);                                     \
+	template int kin_levels_grid<F, Y, T>(int, int, int, int *);                                                      \
+	template int launch_kin_flags<F, Y, T>(const KinSweepParams &, const int2 *, int, int, unsigned *, int *,         \
+										   long long, int *, long long, int, int, int, cudaStream_t);                    \
+	template int kin_flags_grid<F, Y, T>(int, int, int, int *);
 GDN_LEVELS_INST(double, double, double)
 GDN_LEVELS_INST(float, float, float)
 GDN_LEVELS_INST(__nv_bfloat16, float, float)

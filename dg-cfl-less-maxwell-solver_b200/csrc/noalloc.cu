@@ -126,7 +126,8 @@ extern "C" int gdn_cuda_error_l2_noalloc(const double *w, const double *xyz, con
 					  nbelems, (long long)kNoAllocMaxBlocks * kNoAllocBlockElems);
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, buf);
 	}
-	if (data->kind != GDN_CUDA_DATA_PLANE && data->kind != GDN_CUDA_DATA_CAVITY)
+	if (data->kind != GDN_CUDA_DATA_PLANE && data->kind != GDN_CUDA_DATA_CAVITY &&
+		data->kind != GDN_CUDA_DATA_STATIONARY)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "error_l2_noalloc: unknown analytic data kind");
 	int dev = 0;
 	GDN_CUDA_TRY(cudaGetDevice(&dev));

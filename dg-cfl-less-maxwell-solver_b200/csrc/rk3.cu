@@ -209,11 +209,23 @@ __device__ __forceinline__ unsigned smem_u32(const void *p)
 {
 	return (unsigned)__cvta_generic_to_shared(p);
 }
-// one value global -> shared, asynchronous (no register holds it meanwhile)
-template <typename T>
-__device__ __forceinline__ void cp_async_value(T *dst, const T *src)
+// six values global -> shared, asynchronously: dst[cc * DS] = src[cc * SS]
+// for cc < 6.  The strides are compile-time, so the six copies address off
+// one shared and one global base register with immediate offsets (separate
+// asm statements would each materialise both addresses).
+template <typename T, int DS, int SS>
+__device__ __forceinline__ void cp_async_6(T *dst, const T *src)
 {
-	asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(sizeof(T))
+	asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n\t"
+				 "cp.async.ca.shared.global [%0+%3], [%1+%4], %2;\n\t"
+				 "cp.async.ca.shared.global [%0+%5], [%1+%6], %2;\n\t"
+				 "cp.async.ca.shared.global [%0+%7], [%1+%8], %2;\n\t"
+				 "cp.async.ca.shared.global [%0+%9], [%1+%10], %2;\n\t"
+				 "cp.async.ca.shared.global [%0+%11], [%1+%12], %2;" ::"r"(smem_u32(dst)),
+				 "l"(src), "n"(sizeof(T)), "n"(1 * DS * (int)sizeof(T)), "n"(1 * SS * (int)sizeof(T)),
+				 "n"(2 * DS * (int)sizeof(T)), "n"(2 * SS * (int)sizeof(T)), "n"(3 * DS * (int)sizeof(T)),
+				 "n"(3 * SS * (int)sizeof(T)), "n"(4 * DS * (int)sizeof(T)), "n"(4 * SS * (int)sizeof(T)),
+				 "n"(5 * DS * (int)sizeof(T)), "n"(5 * SS * (int)sizeof(T))
 				 : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all()
@@ -276,6 +288,38 @@ __device__ __forceinline__ void upwind_flux_h(const T wL[6], const T wR[6], cons
 	F[3] = (h[1] * sE[2] - h[2] * sE[1]) + r2 * (n[0] * nH - nn * dH[0]);
 	F[4] = (h[2] * sE[0] - h[0] * sE[2]) + r2 * (n[1] * nH - nn * dH[1]);
 	F[5] = (h[0] * sE[1] - h[1] * sE[0]) + r2 * (n[2] * nH - nn * dH[2]);
+}
+
+// FP32: the same flux with the (E_k, H_k) component pairs in packed FP32x2
+// arithmetic: d = wR - wL and t_k = n_k (n . d) - |n|^2 d_k per pair, the
+// cross products from the swapped sums (sH_k, sE_k):
+// (F_E, F_H)_k = (1, -1) (h_{k+2} sw_{k+1} - h_{k+1} sw_{k+2}) + r2 t_k.
+template <>
+__device__ __forceinline__ void upwind_flux_h<float>(const float wL[6], const float wR[6], const float n[3],
+													 float F[6])
+{
+	const float nn = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+	const float r2 = 0.5f * inv_norm_eps(nn);
+	const float2 m1 = make_float2(-1.f, -1.f);
+	float2 d[3], sw[3];
+#pragma unroll
+	for (int k = 0; k < 3; k++) {
+		d[k] = __ffma2_rn(make_float2(wL[k], wL[3 + k]), m1, make_float2(wR[k], wR[3 + k]));
+		sw[k] = __fadd2_rn(make_float2(wR[3 + k], wR[k]), make_float2(wL[3 + k], wL[k]));
+	}
+	const float2 nd = __ffma2_rn(make_float2(n[2], n[2]), d[2],
+								 __ffma2_rn(make_float2(n[1], n[1]), d[1], __fmul2_rn(make_float2(n[0], n[0]), d[0])));
+	const float2 mnn = make_float2(-nn, -nn), rr = make_float2(r2, r2), pm = make_float2(1.f, -1.f);
+#pragma unroll
+	for (int k = 0; k < 3; k++) {
+		const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+		const float h1 = 0.5f * n[k1], h2 = 0.5f * n[k2];
+		const float2 t = __ffma2_rn(mnn, d[k], __fmul2_rn(make_float2(n[k], n[k]), nd));
+		const float2 u = __ffma2_rn(make_float2(-h1, -h1), sw[k2], __fmul2_rn(make_float2(h2, h2), sw[k1]));
+		const float2 Fk = __ffma2_rn(u, pm, __fmul2_rn(rr, t));
+		F[k] = Fk.x;
+		F[3 + k] = Fk.y;
+	}
 }
 
 // One tile of 32 elements, phases 1-3 (all threads of the CTA call it: it
@@ -341,14 +385,10 @@ __device__ __forceinline__ void rk3_tile(const Rk3Params<T> &p, long long tile, 
 					const unsigned qn = ((unsigned)pmk[f] >> (4 * warp)) & 15u;
 					const T *g = p.idx32 ? p.w_in + (((unsigned)nbv >> 5) * 1920u + qn * 192u + ((unsigned)nbv & 31u))
 										 : p.w_in + rk3_tix(nbv, (int)qn * 6);
-#pragma unroll
-					for (int cc = 0; cc < 6; cc++)
-						cp_async_value<T>(d + cc * P, g + cc * 32);
+					cp_async_6<T, P, 32>(d, g);
 				} else {
 					const T *g = p.btrace + ((long long)(-nbv - 1) * 6 + warp) * 6;
-#pragma unroll
-					for (int cc = 0; cc < 6; cc++)
-						cp_async_value<T>(d + cc * P, g + cc);
+					cp_async_6<T, P, 1>(d, g);
 				}
 			}
 		}

@@ -72,10 +72,16 @@ typedef struct gdn_cuda_tables {
  * the error norm).  The reference passes a host callback
  * (gdn_model.get_imposed_data, src/models/model.h:24-25); the GPU path needs
  * a descriptor instead.  PLANE: E = amp pol sin(kmag (khat.x - t) + phase),
- * H = khat x E.  CAVITY: maxwell_imposed_macro_cavity
- * (src/models/maxwell.c:118-133) with its constants. */
+ * H = khat x E (the examples' cos wave, examples/rk3_maxwell_plane_wave.c
+ * :35-47, is khat = (1,0,0), pol = (0,0,1), kmag = pi, phase = pi/2).
+ * CAVITY: maxwell_imposed_macro_cavity (src/models/maxwell.c:118-133) with
+ * its constants.  STATIONARY: maxwell_imposed_stationary
+ * (src/models/maxwell.c:16-84); khat, kmag, pol, amp and phase are unused
+ * for CAVITY and STATIONARY.  gdn_cuda_eval_data evaluates a descriptor on
+ * the device, so that a host can check it against its callback. */
 #define GDN_CUDA_DATA_PLANE 0
 #define GDN_CUDA_DATA_CAVITY 1
+#define GDN_CUDA_DATA_STATIONARY 2
 typedef struct gdn_cuda_data {
 	int kind;
 	double khat[3];
@@ -128,8 +134,11 @@ typedef struct gdn_cuda_config {
 	int device; /* CUDA device ordinal */
 	int kin_sweep; /* kinetic transport solve: 1 = a launch per sweep level,
 	                  2 = one cooperative launch walking all levels with a
-	                  grid barrier between them, 0 = the faster of the two,
-	                  timed at attach and cached per (precision, size) */
+	                  grid barrier between them, 3 = one launch driven by
+	                  per-item readiness flags (CTAs take 32-item chunks in
+	                  sweep order and wait only for their upwind neighbours),
+	                  0 = the fastest of the three, timed at attach and cached
+	                  per (precision, size) */
 } gdn_cuda_config;
 
 typedef struct gdn_cuda_handle gdn_cuda_handle;
@@ -162,6 +171,15 @@ int gdn_cuda_mesh_build_gpu(int nbnodes, const double *coords, int nbelems,
 							int *nboundaryfaces, int *nbqnodes, int *face2elem,
 							int *fnode2enode, int *boundaryface, int *elem2qnode,
 							double *node, int device);
+
+/* Evaluates the analytic data `d` on CUDA device `device` with the same
+ * device code the solver uses (boundary values, initial data, error norm):
+ * w[6*i + c] = component c at point xyz[3*i .. 3*i+2] and time t, for i <
+ * npts; xyz and w are host arrays.  No counterpart in the reference: a host
+ * compares the result with its gdn_model.get_imposed_data callback
+ * (src/models/model.h:24-25) before it trusts the descriptor. */
+int gdn_cuda_eval_data(const gdn_cuda_data *d, long long npts, const double *xyz, double t, double *w,
+					   int device);
 
 /* h_min = min over elements of volume / surface (mesh_get_t4_hmin,
  * src/mesh/mesh.c:149-210). */
@@ -297,8 +315,17 @@ int gdn_cuda_space_convergence(const gdn_cuda_mesh *const *meshes, int nb_run,
 /* ---- introspection ------------------------------------------------------ */
 int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
 int gdn_cuda_num_instances(gdn_cuda_handle *h, int *ninst);
-/* kinetic: the sweep mode in use (1 or 2, see kin_sweep; 0 for RK3) */
+/* kinetic: the sweep mode in use (1, 2 or 3, see kin_sweep; 0 for RK3) */
 int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode);
+/* Test and diagnostics hook, no counterpart in the reference: the number of
+ * polls after which a bounded device-side wait (the cooperative sweep's grid
+ * barrier, the flag-driven sweep's readiness waits) gives up, sets the
+ * handle's error flag and lets its launch end; the next call that reads the
+ * state back (get_state, solve, step_host, error_l2, save_xdmf) then returns
+ * GDN_CUDA_ERR_TIMEOUT and the state is invalid until it is set again.
+ * Default 2^21 polls (about a second); 0 gives up at the first poll that
+ * finds its condition unmet.  Captured step loops are rebuilt. */
+int gdn_cuda_set_wait_limit(gdn_cuda_handle *h, long long polls);
 /* RK3: the stage-kernel variant in use (1 or 2, see rk3_variant; 0 for the
  * kinetic scheme) and the resident CTAs per SM it was compiled for (may be
  * NULL) */

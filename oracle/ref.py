@@ -18,7 +18,9 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 SCHEME_RK3, SCHEME_D3Q4, SCHEME_D3Q6 = 0, 1, 2
 SCHEME_RK3_METAL = 3  # RK3 with the metal boundary flux (maxwell.c:205-223)
-DATA_PLANE, DATA_CAVITY = 0, 1
+# analytic data of ref_driver.c: the plane wave, the reference's cavity and
+# stationary data, the examples' cos wave (examples/rk3_maxwell_plane_wave.c:35-47)
+DATA_PLANE, DATA_CAVITY, DATA_STATIONARY, DATA_EXAMPLE_COS = 0, 1, 2, 3
 
 
 class RefData(C.Structure):
@@ -89,6 +91,13 @@ def lib(variant: str = "zero"):
     L.ref_error_l2.argtypes = [vp, C.c_int, C.POINTER(RefData), dp, C.c_double]
     L.ref_init_state.argtypes = [vp, C.c_int, C.POINTER(RefData), dp]
     L.ref_t10_tables.argtypes = [dp, dp, dp, dp, dp, dp, ip]
+    L.ref_msh_read_raw.argtypes = [C.c_char_p, ip, ip, dp, ip]
+    L.ref_eval_data.argtypes = [C.POINTER(RefData), C.c_int, dp, C.c_double, dp]
+    if variant == "bound":
+        L.ref_run_bound.restype = C.c_int
+        L.ref_run_bound.argtypes = [vp, C.c_int, C.POINTER(RefData), vp, C.c_int, C.c_double, C.c_int,
+                                    dp, dp, dp, dp]
+        L.ref_bound_message.restype = C.c_char_p
     _libs[variant] = L
     return L
 
@@ -147,6 +156,21 @@ class RefMesh:
         return dict(wn=wn, t=t.value, err=err.value, cpu_run=crun.value,
                     cpu_asm=casm.value)
 
+    def run_bound(self, scheme, data: RefData, gpu_data, dt: float, steps: int, precision: int = 0):
+        """The reference's flow through the product's binding (variant
+        "bound" only): simulation_init, simulation_set_time_parameters,
+        dg_cuda_attach(gpu_data: a gdon3d_cuda gdn_cuda_data), dg_solve routed
+        to the GPU, simulation_error_l2.  Returns dict(rc, msg, wn, t, err,
+        mismatch)."""
+        wlen = self.L.ref_wlen(self.h, scheme)
+        wn = np.zeros(wlen, np.float64)
+        t, err, mis = (C.c_double() for _ in range(3))
+        with _stdout_to_stderr():
+            rc = self.L.ref_run_bound(self.h, scheme, C.byref(data), C.cast(C.byref(gpu_data), C.c_void_p),
+                                      precision, dt, steps, _dp(wn), C.byref(t), C.byref(err), C.byref(mis))
+        return dict(rc=rc, msg=self.L.ref_bound_message().decode(), wn=wn, t=t.value, err=err.value,
+                    mismatch=mis.value)
+
     def error_l2(self, scheme, data: RefData, wn: np.ndarray, t: float) -> float:
         w = np.ascontiguousarray(wn, dtype=np.float64)
         return float(self.L.ref_error_l2(self.h, scheme, C.byref(data), _dp(w), t))
@@ -166,6 +190,28 @@ class RefMesh:
             self.close()
         except Exception:
             pass
+
+
+def eval_callback(kind: int, xyz: np.ndarray, t: float, variant: str = "zero", **kw) -> np.ndarray:
+    """The reference-side callback of data `kind` (ref_driver.c select_data)
+    at points xyz[n, 3] and time t: [n, 6]."""
+    x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    w = np.zeros((len(x), 6))
+    lib(variant).ref_eval_data(C.byref(make_data(kind=kind, **kw)), len(x), _dp(x), float(t), _dp(w))
+    return w
+
+
+def msh_read_raw(path: str, variant: str = "zero"):
+    """(coords[n, 3], elem2node[ne, 4] 0-based) of a msh22 file as the
+    reference's reader leaves them (T4 elements only, no connectivity)."""
+    L = lib(variant)
+    nn, ne = C.c_int(), C.c_int()
+    with _stdout_to_stderr():
+        L.ref_msh_read_raw(path.encode(), C.byref(nn), C.byref(ne), None, None)
+        coords = np.zeros((nn.value, 3))
+        e2n = np.zeros((ne.value, 4), np.int32)
+        L.ref_msh_read_raw(path.encode(), C.byref(nn), C.byref(ne), _dp(coords), _ip(e2n))
+    return coords, e2n
 
 
 def t10_tables(variant: str = "zero"):

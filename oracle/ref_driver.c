@@ -11,10 +11,18 @@
  * dg_solve (src/dg/dg.c:23) and simulation_error_l2
  * (src/simulation/simulation.c:606) and hands back the final state vector.
  *
- * The only analytic data functions defined here are the plane wave of the
- * benchmark configurations (a new data set, not in the reference); the PEC
- * cavity uses the reference's maxwell_imposed_macro_cavity
- * (src/models/maxwell.c:118-133) directly.
+ * The analytic data defined here are the plane wave of the benchmark
+ * configurations (a new data set, not in the reference) and the examples'
+ * cos wave (imposed_macro_cos, a static function of
+ * examples/rk3_maxwell_plane_wave.c:35-47 and
+ * examples/relax_maxwell_plane_wave.c:35-47, restated); the PEC cavity and
+ * the stationary data use the reference's maxwell_imposed_macro_cavity and
+ * maxwell_imposed_stationary (src/models/maxwell.c:118-133, 72-84) directly.
+ *
+ * Built a third time with GDN_REF_BOUND defined (libgdon3d_ref_bound.so):
+ * the reference's dg.c renamed dg_solve -> dg_solve_host and the product's
+ * binding integration/dg_cuda.c linked in, so that ref_run_bound drives the
+ * reference's own flow with dg_solve routed to the GPU.
  */
 #include <math.h>
 #include <stdbool.h>
@@ -33,8 +41,13 @@
 #include <simulation/simulation.h>
 
 /* analytic data descriptor (same meaning as the product's gdn_cuda_data) */
+#ifdef GDN_REF_BOUND
+#include "../integration/dg_cuda.h"
+#endif
+
 typedef struct ref_data {
-	int kind; /* 0 plane wave, 1 PEC cavity (reference formula) */
+	int kind; /* 0 plane wave, 1 PEC cavity, 2 stationary (reference formulas),
+	             3 the examples' cos wave */
 	double khat[3];
 	double kmag;
 	double pol[3];
@@ -62,11 +75,27 @@ static void plane_wave(const gdn_real *x, const gdn_real t, gdn_real *w)
 	w[5] = hz * s;
 }
 
+/* the examples' data: Ez = cos(pi (x - t)), Hy = -Ez */
+static void example_cos(const gdn_real *x, const gdn_real t, gdn_real *w)
+{
+	const gdn_real s = cos(1 * M_PI * (x[0] - t));
+	w[0] = 0;
+	w[1] = 0;
+	w[2] = s;
+	w[3] = 0;
+	w[4] = -s;
+	w[5] = 0;
+}
+
 static gdn_get_imposed_data select_data(const ref_data *d)
 {
 	g_data = *d;
 	if (d->kind == 1)
 		return maxwell_imposed_macro_cavity;
+	if (d->kind == 2)
+		return maxwell_imposed_stationary;
+	if (d->kind == 3)
+		return example_cos;
 	return plane_wave;
 }
 
@@ -95,6 +124,36 @@ void *ref_mesh_from_arrays(int nbnodes, const double *coords, int nbelems,
 	m->elem2elem = NULL;
 	mesh_build_connectivity(m);
 	return m;
+}
+
+/* The T4 content of a msh22 file as the reference's reader leaves it
+ * (src/mesh/mesh.c:623-726, no connectivity): call with NULL arrays for the
+ * sizes, then with coords[3*nbnodes] and elem2node[4*nbelems] (0-based). */
+int ref_msh_read_raw(const char *path, int *nbnodes, int *nbelems, double *coords, int *elem2node)
+{
+	gdn_mesh m;
+	memset(&m, 0, sizeof(m));
+	mesh_read_from_msh22_file(&m, path);
+	*nbnodes = m.nbnodes;
+	*nbelems = m.nbelems;
+	if (coords)
+		memcpy(coords, m.node, sizeof(double) * 3 * m.nbnodes);
+	if (elem2node)
+		memcpy(elem2node, m.elem2node, sizeof(int) * 4 * m.nbelems);
+	free(m.node);
+	free(m.elem2node);
+	if (m.physical_group_is_alloc)
+		free(m.physical_group);
+	return 0;
+}
+
+/* The host callback of data `d` (what model->get_imposed_data returns) at n
+ * points and time t: w[6*i + c]. */
+void ref_eval_data(const ref_data *d, int n, const double *xyz, double t, double *w)
+{
+	gdn_get_imposed_data fn = select_data(d);
+	for (int i = 0; i < n; i++)
+		fn(xyz + 3 * i, t, w + 6 * i);
 }
 
 void ref_mesh_info(void *pm, int *out)
@@ -255,3 +314,48 @@ void ref_t10_tables(double *wpg, double *mass, double *inv_mass,
 			face2node[6 * f + j] = t10_get_ref_face2node_entry(f, j);
 	}
 }
+
+#ifdef GDN_REF_BOUND
+/* The reference's flow with the GPU binding: simulation_init,
+ * simulation_set_time_parameters, dg_cuda_attach (gd, FP64 or another
+ * precision), dg_solve (routed to the GPU), simulation_error_l2 on the state
+ * written back.  Returns the attach status (the message through
+ * ref_bound_message), or the routed solve's status. */
+int ref_run_bound(void *pm, int scheme, const ref_data *d, const gdn_cuda_data *gd, int precision, double dt,
+				  int steps, double *wn_out, double *t_out, double *err_out, double *mismatch_out)
+{
+	gdn_mesh *m = (gdn_mesh *)pm;
+	gdn_model model;
+	gdn_simulation simu;
+	memset(&simu, 0, sizeof(simu));
+	setup_model(&model, scheme, d);
+	simulation_init(m, &model, &simu);
+	simulation_set_time_parameters(&simu, (steps + 0.5) * dt, dt, -1);
+	if (simu.itermax != steps) {
+		free(simu.wn);
+		return -1;
+	}
+	gdn_cuda_config cfg = {precision, 1, 0, 1, 0, 0};
+	int rc = dg_cuda_attach(&simu, gd, &cfg);
+	if (mismatch_out)
+		*mismatch_out = dg_cuda_data_mismatch();
+	if (rc == 0) {
+		dg_solve(&simu);
+		rc = dg_cuda_status(&simu);
+		if (wn_out)
+			memcpy(wn_out, simu.wn, sizeof(double) * simu.wlen);
+		if (t_out)
+			*t_out = simu.t;
+		if (err_out)
+			*err_out = simulation_error_l2(&simu);
+		dg_cuda_detach(&simu);
+	}
+	free(simu.wn);
+	return rc;
+}
+
+const char *ref_bound_message(void)
+{
+	return dg_cuda_message();
+}
+#endif

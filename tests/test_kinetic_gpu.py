@@ -172,23 +172,69 @@ def test_kinetic_bf16_storage_error_is_bounded():
 
 @pytest.mark.parametrize("precision,nb_v", [(capi.FP64, 4), (capi.FP32, 6), (capi.FP32_REFINE, 4),
                                             (capi.BF16_STORE, 4)])
-def test_kinetic_cooperative_sweep_equals_level_launches(precision, nb_v):
+def test_kinetic_sweep_modes_equal_level_launches(precision, nb_v):
     """One cooperative launch walking all sweep levels (grid barrier between
-    levels) does per item the arithmetic of one launch per level: identical
-    states."""
+    levels) and one flag-driven launch (each chunk waits for its upwind
+    neighbours' readiness flags) do per item the arithmetic of one launch per
+    level: identical states."""
     c, e = kuhn.kuhn_cube(5, 0.15, seed=8)
     mesh = capi.mesh_build(c, e)
     dt = 10 * 0.3 * mesh.hmin()
     out = []
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, precision=precision, nb_v=nb_v,
                         kin_sweep=mode)
         assert s.kin_sweep_mode == mode
         wn, t, _ = s.solve(6)
         out.append((wn, t, s.error_l2()))
         s.close()
-    assert np.array_equal(out[0][0], out[1][0])
-    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0])
+        assert out[0][1] == o[1] and out[0][2] == o[2]
+
+
+def test_kinetic_flag_sweep_cavity_16_matches_reference():
+    """The flag-driven sweep on the plain CFL-less workload (16^3 x 6 cavity,
+    10 x CFL, d3q4) against the reference build, 30 steps."""
+    c, e = kuhn.kuhn_cube(16, 0.0, seed=5)
+    mesh = capi.mesh_build(c, e)
+    dt = 10 * 0.3 * mesh.hmin()
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, kin_sweep=3)
+    assert s.kin_sweep_mode == 3
+    wn, t, _ = s.solve(30)
+    s.close()
+    r = ref.RefMesh(c, e).run(ref.SCHEME_D3Q4, ref.make_data(kind=ref.DATA_CAVITY), dt, 30)
+    rel = np.linalg.norm(wn - r["wn"]) / np.linalg.norm(r["wn"])
+    assert rel <= 1e-12, rel
+    assert t == r["t"]
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+def test_kinetic_bounded_wait_gives_up_with_timeout_status(mode):
+    """A device-side wait whose limit runs out ends its launch and reports
+    GDN_CUDA_ERR_TIMEOUT at the next call that reads the state; the context
+    stays usable and, with the limit restored, the same handle solves
+    correctly.  The limit is 0 polls: every wait whose condition is not met
+    at its first poll gives up, which on a mesh of 80 sweep levels happens in
+    the first levels (a flag that is not yet set, or CTAs still to arrive)."""
+    c, e = kuhn.kuhn_cube(12, 0.1, seed=3)
+    mesh = capi.mesh_build(c, e)
+    dt = 10 * 0.3 * mesh.hmin()
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, kin_sweep=mode)
+    assert s.num_levels > 40
+    s.set_wait_limit(0)
+    s.init()
+    s.advance(3)
+    with pytest.raises(capi.GdnError) as ex:
+        s.get_state()
+    assert ex.value.code == capi.ERR_TIMEOUT
+    s.set_wait_limit(1 << 21)
+    wn, t, _ = s.solve(3)
+    s.close()
+    s1 = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, kin_sweep=1)
+    w1, t1, _ = s1.solve(3)
+    s1.close()
+    assert np.array_equal(wn, w1) and t == t1
 
 
 @pytest.mark.parametrize("n,levels", [(16, 108), (64, 444)])
