@@ -37,7 +37,17 @@ def test_reference_progress_prints_stay_off_stdout(capfd):
 
 
 def test_rk3_algorithmic_bytes():
-    # 600 state values x b_s + 3 stages x (10 geometry values x b_g + 32 bytes of neighbour rows)
-    assert bench.algorithmic_bytes_per_step(1, 4, 4) == 600 * 4 + 3 * (40 + 32)
-    assert bench.algorithmic_bytes_per_step(1, 8, 8) == 600 * 8 + 3 * (80 + 32)
-    assert bench.algorithmic_bytes_per_step(5308416, 4, 4) == 5308416 * 2616
+    # the scope table's figure per element and step: 660 b_s + 30 b_g + 60
+    # (FP64 5,580 B, FP32 2,820 B)
+    assert bench.algorithmic_bytes_per_step(1, 4, 4) == 2820
+    assert bench.algorithmic_bytes_per_step(1, 8, 8) == 5580
+    assert bench.algorithmic_bytes_per_step(5308416, 4, 4) == 5308416 * 2820
+    # the kernel's own minimum: k2 not written in the last stage, 32-byte records
+    assert bench.tight_bytes_per_step(1, 4, 4) == 600 * 4 + 3 * (40 + 32) == 2616
+    assert bench.tight_bytes_per_step(1, 8, 8) == 600 * 8 + 3 * (80 + 32) == 5136
+
+
+def test_kinetic_algorithmic_bytes():
+    # 2 x 240 b_s + 10 b_g + 20 per element and step
+    assert bench.kinetic_algorithmic_bytes(1, 4, 4) == 2 * 240 * 4 + 40 + 20
+    assert bench.kinetic_algorithmic_bytes(1, 8, 8) == 2 * 240 * 8 + 80 + 20
