@@ -327,6 +327,10 @@ def main():
     ap.add_argument("--only", default="all",
                     help="profiling aid: comma-separated variants to run (rk3: fp64,fp32; kinetic: "
                          "fp64,fp32,fp32_refine1,fp32_refine2,bf16)")
+    ap.add_argument("--kin-sweep", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="kinetic: force the sweep mode (1 level launches, 2 cooperative, 3 readiness "
+                         "flags, 4 spatial parts) and skip the per-mode timing; 0 = autotuned, with the "
+                         "per-mode timing")
     ap.add_argument("--headline-only", action="store_true",
                     help="rk3: print the 96^3 line without the kinetic precision study and the batch")
     args = ap.parse_args()
@@ -552,7 +556,7 @@ def run_kinetic(args, env):
         if not _wanted(args, name):
             continue
         s = capi.Solver(mesh, capi.SCHEME_KINETIC, data, dt, precision=prec, refine_passes=passes, nb_v=4,
-                        device=env.local)
+                        device=env.local, kin_sweep=args.kin_sweep)
         s.init()
         s.advance(W)  # warm-up, captures the step graph
         s.init()
@@ -587,10 +591,11 @@ def run_kinetic(args, env):
     # (the variants above run the one the autotuner picked)
     sweep_modes = {}
     for name, prec in (("fp64", capi.FP64), ("fp32", capi.FP32)):
-        if not _wanted(args, name):
+        if not _wanted(args, name) or args.kin_sweep:
             continue
         sweep_modes[name] = {}
-        for mode, label in ((1, "level_launches"), (2, "cooperative_grid_barrier"), (3, "readiness_flags")):
+        for mode, label in ((1, "level_launches"), (2, "cooperative_grid_barrier"), (3, "readiness_flags"),
+                            (4, "spatial_parts")):
             s = capi.Solver(mesh, capi.SCHEME_KINETIC, data, dt, precision=prec, nb_v=4, device=env.local,
                             kin_sweep=mode)
             s.init()
@@ -735,7 +740,7 @@ def run_batched(args, env, specs, built):
                    "seed": SEED, "rk3_steps": BATCH_RK3_STEPS, "kinetic_steps": BATCH_KIN_STEPS,
                    "kinetic_cfl_multiple": BATCH_KIN_MULT, "rk3_variant_autotuned": tile,
                    "kinetic_sweep_mode_autotuned": {1: "level_launches", 2: "cooperative_grid_barrier",
-                                                    3: "readiness_flags"}.get(kmode, kmode),
+                                                    3: "readiness_flags", 4: "spatial_parts"}.get(kmode, kmode),
                    "kinetic_levels": levels, "attach_s": attach_s,
                    "precision": "FP32 state and arithmetic; FP64 setup and norms",
                    "l2_flush": "inputs larger than L2 (%.1f GB of FP32 RK3 state)"

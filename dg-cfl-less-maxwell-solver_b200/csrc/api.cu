@@ -18,6 +18,7 @@ namespace gdn {
 template <typename GT>
 int launch_kin_setup(const int *face2elem, long long nf, const double *geom, const int *nb, long long ne,
 					 const KinModel &km, double *sown64, unsigned char *mask, cudaStream_t s);
+int kin_upload_block_tables(const gdn_cuda_tables *t);
 template <typename GT>
 int launch_kin_blocks(const double *geom, const double *sown64, const int *items, const int *pos, const int *nb,
 					  const int *perm, long long ne, const KinModel &km, double theta, const int *einst,
@@ -112,7 +113,8 @@ struct gdn_cuda_handle {
 	double *yacc = nullptr; // FP32_REFINE: FP64 solution of the transport solve
 	float *rhs = nullptr; // FP32_REFINE: residual, right-hand side of the corrections
 	int refine_passes = 1;
-	int kin_mode = 1; // 1: a launch per sweep level, 2: one cooperative launch per sweep, 3: flag-driven
+	int kin_mode = 1; // 1: a launch per sweep level, 2: one cooperative launch per sweep, 3: flag-driven,
+	                  // 4: spatial parts
 	bool kin_autotune = true; // pick kin_mode at attach by timing the modes
 	int kin_grid[3] = {0, 0, 0}; // CTAs of the cooperative sweep, per accumulate mode
 	int kin_fgrid[3] = {0, 0, 0}; // CTAs of the flag-driven sweep, per accumulate mode
@@ -121,6 +123,12 @@ struct gdn_cuda_handle {
 	int *kready = nullptr; // [nitems] readiness flags of the flag-driven sweep
 	unsigned *kqueue = nullptr; // its chunk counter
 	long long spin_limit = 1LL << 21; // polls of a bounded device-side wait (~1 s)
+	// the spatial-parts sweep: item list by part, level-aligned chunks, chunk ranges per part
+	int *plist = nullptr;
+	int2 *pchunks = nullptr;
+	int *part_chunk_off = nullptr;
+	int nparts = 0;
+	int kin_pgrid[3] = {0, 0, 0}; // CTAs of the parts sweep that fit at once, per accumulate mode
 	int max_chunks = 1; // most 32-item chunks in one level
 	int *level_off_dev = nullptr;
 	unsigned *bar = nullptr; // [2] grid barrier of the cooperative sweep
@@ -468,6 +476,7 @@ static int autotune_rk3(gdn_cuda_handle *h)
 }
 
 static int kin_prepare_grids(gdn_cuda_handle *h);
+static int kin_prepare_parts(gdn_cuda_handle *h, const gdn_cuda_mesh *m);
 static int autotune_kin(gdn_cuda_handle *h);
 
 static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cuda_tables *t,
@@ -617,6 +626,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 			GDN_TRY(dalloc(h, &h->ru64, nu));
 			GDN_TRY(dalloc(h, &h->rs64, nu));
 		}
+		GDN_TRY(kin_upload_block_tables(t));
 		if (fp64) {
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->G), 100 * nu));
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->rs), 4 * nu));
@@ -664,6 +674,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		GDN_TRY(dalloc(h, &h->kready, nu));
 		GDN_TRY(dalloc(h, &h->kqueue, 1));
 		GDN_TRY(kin_prepare_grids(h));
+		GDN_TRY(kin_prepare_parts(h, m));
 		GDN_CUDA_TRY(cudaStreamSynchronize(s));
 		if (h->kin_autotune)
 			GDN_TRY(autotune_kin(h));
@@ -809,8 +820,8 @@ static int attach_batch(const gdn_cuda_instance *inst, int n, const gdn_cuda_tab
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: unknown precision mode");
 	if (cfg.rk3_variant < 0 || cfg.rk3_variant > 2)
 		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: rk3_variant must be 0 (auto), 1 or 2");
-	if (cfg.kin_sweep < 0 || cfg.kin_sweep > 3)
-		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kin_sweep must be 0 (auto), 1, 2 or 3");
+	if (cfg.kin_sweep < 0 || cfg.kin_sweep > 4)
+		return gdn_set_error(GDN_CUDA_ERR_INVALID, "attach: kin_sweep must be 0 (auto), 1, 2, 3 or 4");
 	for (int i = 0; i < n; i++) {
 		GDN_TRY(validate_mesh(inst[i].mesh));
 		GDN_TRY(validate_data(inst[i].data));
@@ -993,6 +1004,15 @@ static int kin_sweeps(gdn_cuda_handle *h, const void *f, int acc, int bdata, lon
 		nlaunch++;
 		return GDN_CUDA_OK;
 	}
+	if (h->kin_mode == 4) {
+		p.item_begin = 0;
+		p.item_end = h->level_off[nl];
+		GDN_TRY((launch_kin_parts<F, Y, T>(p, h->plist, h->pchunks, h->part_chunk_off, h->nparts, h->kready,
+										   h->ne * h->nv, h->err, h->spin_limit, acc, bdata, h->rk3_sparse,
+										   h->stream)));
+		nlaunch++;
+		return GDN_CUDA_OK;
+	}
 	if (h->kin_mode == 3) {
 		p.item_begin = 0;
 		p.item_end = h->level_off[nl];
@@ -1105,6 +1125,20 @@ static int kin_prepare_grids(gdn_cuda_handle *h)
 	GDN_TRY(kin_prepare_flag_grids(h));
 	switch (h->precision) {
 	case GDN_CUDA_FP64:
+		GDN_TRY((kin_parts_grid<double, double, double>(h->device, 0, sp, &h->kin_pgrid[0])));
+		break;
+	case GDN_CUDA_FP32:
+		GDN_TRY((kin_parts_grid<float, float, float>(h->device, 0, sp, &h->kin_pgrid[0])));
+		break;
+	case GDN_CUDA_BF16_STORE:
+		GDN_TRY((kin_parts_grid<__nv_bfloat16, float, float>(h->device, 0, sp, &h->kin_pgrid[0])));
+		break;
+	default:
+		GDN_TRY((kin_parts_grid<double, float, float>(h->device, 1, sp, &h->kin_pgrid[1])));
+		GDN_TRY((kin_parts_grid<float, float, float>(h->device, 2, sp, &h->kin_pgrid[2])));
+	}
+	switch (h->precision) {
+	case GDN_CUDA_FP64:
 		return kin_levels_grid<double, double, double>(h->device, 0, sp, &h->kin_grid[0]);
 	case GDN_CUDA_FP32:
 		return kin_levels_grid<float, float, float>(h->device, 0, sp, &h->kin_grid[0]);
@@ -1114,6 +1148,67 @@ static int kin_prepare_grids(gdn_cuda_handle *h)
 		GDN_TRY((kin_levels_grid<double, float, float>(h->device, 1, sp, &h->kin_grid[1])));
 		return kin_levels_grid<float, float, float>(h->device, 2, sp, &h->kin_grid[2]);
 	}
+}
+
+// The spatial parts of the parts sweep: as many parts as CTAs of every
+// launched variant fit at once (at least 32 elements each), the item list by
+// part (device), its level-aligned chunks (at most 32 items) and each part's
+// chunk range.
+static int kin_prepare_parts(gdn_cuda_handle *h, const gdn_cuda_mesh *m)
+{
+	int cap = 0;
+	for (int a = 0; a < 3; a++)
+		if (h->kin_pgrid[a] > 0)
+			cap = cap == 0 || h->kin_pgrid[a] < cap ? h->kin_pgrid[a] : cap;
+	const long long byelem = h->ne / 32 > 0 ? h->ne / 32 : 1;
+	h->nparts = (int)(cap < byelem ? cap : byelem);
+	if (h->nparts < 1)
+		h->nparts = 1;
+	double lo[3] = {m->node[0], m->node[1], m->node[2]}, hi[3] = {m->node[0], m->node[1], m->node[2]};
+	for (long long q = 0; q < h->nq; q++)
+		for (int a = 0; a < 3; a++) {
+			lo[a] = std::fmin(lo[a], m->node[3 * q + a]);
+			hi[a] = std::fmax(hi[a], m->node[3 * q + a]);
+		}
+	const long long nitems = h->ne * h->nv;
+	GDN_TRY(dalloc(h, &h->plist, nitems));
+	std::vector<int> plist, pkey;
+	GDN_TRY(kin_build_parts(h->e2q, h->node, h->ne, lo, hi, h->items, nitems, h->nv, h->nparts, h->rnb, h->rpm,
+							h->plist, plist, pkey, h->stream));
+	h->launches += 5;
+	std::vector<int2> chunks;
+	std::vector<int> off(h->nparts + 1, 0);
+	long long i = 0;
+	for (int b = 0; b < h->nparts; b++) {
+		off[b] = (int)chunks.size();
+		size_t l = 0; // level of the current item (plist is in sweep order within a part)
+		int start = -1, cnt = 0;
+		size_t lstart = 0;
+		for (; i < nitems && pkey[i] == b; i++) {
+			const int k = plist[i];
+			while (l + 1 < h->level_off.size() && k >= h->level_off[l + 1])
+				l++;
+			if (start < 0 || l != lstart || cnt == 32) {
+				if (start >= 0)
+					chunks.push_back(make_int2(start, cnt));
+				start = (int)i;
+				cnt = 0;
+				lstart = l;
+			}
+			cnt++;
+		}
+		if (start >= 0)
+			chunks.push_back(make_int2(start, cnt));
+	}
+	off[h->nparts] = (int)chunks.size();
+	GDN_TRY(dalloc(h, &h->pchunks, chunks.size()));
+	GDN_TRY(dalloc(h, &h->part_chunk_off, off.size()));
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->pchunks, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice,
+								 h->stream));
+	GDN_CUDA_TRY(cudaMemcpyAsync(h->part_chunk_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice,
+								 h->stream));
+	GDN_CUDA_TRY(cudaStreamSynchronize(h->stream));
+	return GDN_CUDA_OK;
 }
 
 // the first transport solve of a step, as the step runs it
@@ -1163,7 +1258,7 @@ static int autotune_kin(gdn_cuda_handle *h)
 	GDN_CUDA_TRY(cudaEventCreate(&ev[1]));
 	float best = 0.f;
 	int pick = 1, rc = GDN_CUDA_OK;
-	for (int mode = 1; mode <= 3 && rc == GDN_CUDA_OK; mode++) {
+	for (int mode = 1; mode <= 4 && rc == GDN_CUDA_OK; mode++) {
 		h->kin_mode = mode;
 		long long nlaunch = 0;
 		rc = kin_first_sweep(h, nlaunch); // warm-up

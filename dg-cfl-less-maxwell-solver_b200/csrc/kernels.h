@@ -115,6 +115,24 @@ int launch_kin_flags(const KinSweepParams &p, const int2 *chunks, int nchunks, i
 template <typename F, typename Y, typename T>
 int kin_flags_grid(int device, int acc, int sparse, int *grid);
 
+// The same solve with each CTA of one cooperative launch sweeping one compact
+// spatial part in sweep order (plist, level-aligned chunks pchunks[c] = first
+// list position and count, part b's chunks from part_chunk_off[b]); only
+// upwind items of other parts (bit 28 of their face's rpm entry) are waited
+// for through ready[] (cleared before the launch).
+template <typename F, typename Y, typename T>
+int launch_kin_parts(const KinSweepParams &p, const int *plist, const int2 *pchunks, const int *part_chunk_off,
+					 int nparts, int *ready, long long nitems, int *err, long long spin_limit, int acc, int bdata,
+					 int sparse, cudaStream_t s);
+template <typename F, typename Y, typename T>
+int kin_parts_grid(int device, int acc, int sparse, int *grid);
+// the parts: elements split into nparts equal ranges along a Morton curve of
+// their centroids (bounding box lo, hi); plist (device) and its host copy,
+// the part of every list entry (host), bit 28 of rpm set for external inflow
+int kin_build_parts(const int *e2q, const double *node, long long ne, const double lo[3], const double hi[3],
+					const int *items, long long nitems, int nv, int nparts, const int4 *rnb, int4 *rpm, int *plist,
+					std::vector<int> &plist_host, std::vector<int> &pkey_host, cudaStream_t s);
+
 // Level schedule of the upwind item graph on the device: items[k] (e * nv +
 // v in level order, ascending within a level), pos (its inverse), level_off
 // (host, first item of each level, then the item count); GDN_CUDA_ERR_CYCLE

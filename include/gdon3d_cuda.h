@@ -137,7 +137,10 @@ typedef struct gdn_cuda_config {
 	                  grid barrier between them, 3 = one launch driven by
 	                  per-item readiness flags (CTAs take 32-item chunks in
 	                  sweep order and wait only for their upwind neighbours),
-	                  0 = the fastest of the three, timed at attach and cached
+	                  4 = one cooperative launch in which each CTA sweeps one
+	                  compact spatial part of the mesh in sweep order and
+	                  waits only for upwind items of other parts,
+	                  0 = the fastest of the four, timed at attach and cached
 	                  per (precision, size) */
 } gdn_cuda_config;
 
@@ -315,11 +318,11 @@ int gdn_cuda_space_convergence(const gdn_cuda_mesh *const *meshes, int nb_run,
 /* ---- introspection ------------------------------------------------------ */
 int gdn_cuda_get_time(gdn_cuda_handle *h, double *t);
 int gdn_cuda_num_instances(gdn_cuda_handle *h, int *ninst);
-/* kinetic: the sweep mode in use (1, 2 or 3, see kin_sweep; 0 for RK3) */
+/* kinetic: the sweep mode in use (1 to 4, see kin_sweep; 0 for RK3) */
 int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode);
 /* Test and diagnostics hook, no counterpart in the reference: the number of
  * polls after which a bounded device-side wait (the cooperative sweep's grid
- * barrier, the flag-driven sweep's readiness waits) gives up, sets the
+ * barrier, the flag-driven and spatial-parts sweeps' readiness waits) gives up, sets the
  * handle's error flag and lets its launch end; the next call that reads the
  * state back (get_state, solve, step_host, error_l2, save_xdmf) then returns
  * GDN_CUDA_ERR_TIMEOUT and the state is invalid until it is set again.

@@ -174,14 +174,15 @@ def test_kinetic_bf16_storage_error_is_bounded():
                                             (capi.BF16_STORE, 4)])
 def test_kinetic_sweep_modes_equal_level_launches(precision, nb_v):
     """One cooperative launch walking all sweep levels (grid barrier between
-    levels) and one flag-driven launch (each chunk waits for its upwind
-    neighbours' readiness flags) do per item the arithmetic of one launch per
-    level: identical states."""
+    levels), one flag-driven launch (each chunk waits for its upwind
+    neighbours' readiness flags) and one cooperative launch of spatial parts
+    (each CTA sweeps its part, waiting only for other parts' items) do per
+    item the arithmetic of one launch per level: identical states."""
     c, e = kuhn.kuhn_cube(5, 0.15, seed=8)
     mesh = capi.mesh_build(c, e)
     dt = 10 * 0.3 * mesh.hmin()
     out = []
-    for mode in (1, 2, 3):
+    for mode in (1, 2, 3, 4):
         s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, precision=precision, nb_v=nb_v,
                         kin_sweep=mode)
         assert s.kin_sweep_mode == mode
@@ -193,14 +194,16 @@ def test_kinetic_sweep_modes_equal_level_launches(precision, nb_v):
         assert out[0][1] == o[1] and out[0][2] == o[2]
 
 
-def test_kinetic_flag_sweep_cavity_16_matches_reference():
-    """The flag-driven sweep on the plain CFL-less workload (16^3 x 6 cavity,
-    10 x CFL, d3q4) against the reference build, 30 steps."""
+@pytest.mark.parametrize("mode", [3, 4])
+def test_kinetic_one_launch_sweeps_cavity_16_match_reference(mode):
+    """The flag-driven and the spatial-parts sweeps on the plain CFL-less
+    workload (16^3 x 6 cavity, 10 x CFL, d3q4) against the reference build,
+    30 steps."""
     c, e = kuhn.kuhn_cube(16, 0.0, seed=5)
     mesh = capi.mesh_build(c, e)
     dt = 10 * 0.3 * mesh.hmin()
-    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, kin_sweep=3)
-    assert s.kin_sweep_mode == 3
+    s = capi.Solver(mesh, capi.SCHEME_KINETIC, capi.cavity_data(), dt, kin_sweep=mode)
+    assert s.kin_sweep_mode == mode
     wn, t, _ = s.solve(30)
     s.close()
     r = ref.RefMesh(c, e).run(ref.SCHEME_D3Q4, ref.make_data(kind=ref.DATA_CAVITY), dt, 30)
@@ -209,14 +212,16 @@ def test_kinetic_flag_sweep_cavity_16_matches_reference():
     assert t == r["t"]
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", [2, 3, 4])
 def test_kinetic_bounded_wait_gives_up_with_timeout_status(mode):
     """A device-side wait whose limit runs out ends its launch and reports
     GDN_CUDA_ERR_TIMEOUT at the next call that reads the state; the context
     stays usable and, with the limit restored, the same handle solves
     correctly.  The limit is 0 polls: every wait whose condition is not met
     at its first poll gives up, which on a mesh of 80 sweep levels happens in
-    the first levels (a flag that is not yet set, or CTAs still to arrive)."""
+    the first levels (a flag that is not yet set, or CTAs still to arrive; the
+    spatial-parts sweep has several hundred parts, most of them downstream of
+    others)."""
     c, e = kuhn.kuhn_cube(12, 0.1, seed=3)
     mesh = capi.mesh_build(c, e)
     dt = 10 * 0.3 * mesh.hmin()
