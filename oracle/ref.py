@@ -93,6 +93,9 @@ def lib(variant: str = "zero"):
     L.ref_t10_tables.argtypes = [dp, dp, dp, dp, dp, dp, ip]
     L.ref_msh_read_raw.argtypes = [C.c_char_p, ip, ip, dp, ip]
     L.ref_eval_data.argtypes = [C.POINTER(RefData), C.c_int, dp, C.c_double, dp]
+    L.ref_time_convergence.restype = C.c_int
+    L.ref_time_convergence.argtypes = [C.c_char_p, C.c_int, C.POINTER(RefData), C.c_double, C.c_double,
+                                       C.c_int, C.c_int, vp]
     if variant == "bound":
         L.ref_run_bound.restype = C.c_int
         L.ref_run_bound.argtypes = [vp, C.c_int, C.POINTER(RefData), vp, C.c_int, C.c_double, C.c_int,
@@ -190,6 +193,42 @@ class RefMesh:
             self.close()
         except Exception:
             pass
+
+
+def time_convergence(path: str, scheme: int, data: RefData, init_dt: float, tmax: float, nb_run: int,
+                     variant: str = "zero", gpu_data=None):
+    """The reference's utils_l2_time_convergence on a msh file; with
+    variant "bound" and gpu_data, every dg_solve routed to the GPU through the
+    binding.  Returns the per-run rows it printed: dict(dt, iter, error, order)
+    (order None for the first run)."""
+    import re
+    import tempfile
+    L = lib(variant)
+    with tempfile.TemporaryFile(mode="w+") as out:
+        import sys
+        sys.stdout.flush()
+        _libc.fflush(None)
+        saved = os.dup(1)
+        os.dup2(out.fileno(), 1)
+        try:
+            rc = L.ref_time_convergence(path.encode(), scheme, C.byref(data), init_dt, tmax, nb_run,
+                                        1 if gpu_data is not None else 0,
+                                        C.cast(C.byref(gpu_data), C.c_void_p) if gpu_data is not None else None)
+        finally:
+            _libc.fflush(None)
+            os.dup2(saved, 1)
+            os.close(saved)
+        out.seek(0)
+        text = out.read()
+    if rc != 0:
+        raise RuntimeError("reference convergence driver: status %d" % rc)
+    rows = []
+    for line in re.split(r"[\r\n]+", text):
+        f = line.split()
+        if len(f) == 12 and f[0] == "fooo":
+            rows.append(dict(dt=float(f[6]), iter=int(f[3]), error=float(f[10]),
+                             order=None if f[11] == "---" else float(f[11])))
+    return rows
 
 
 def eval_callback(kind: int, xyz: np.ndarray, t: float, variant: str = "zero", **kw) -> np.ndarray:

@@ -41,9 +41,30 @@
 #include <simulation/simulation.h>
 
 /* analytic data descriptor (same meaning as the product's gdn_cuda_data) */
+#include <utils/convergence.h>
+
 #ifdef GDN_REF_BOUND
 #include "../integration/dg_cuda.h"
 #endif
+
+/* The reference's io_save_all (src/io/io_hdf5.c:355-368) needs libhdf5, which is
+ * not installed, so io_hdf5.c is not compiled; utils_l2_time_convergence
+ * (src/utils/convergence.c) still names it.  In the bound library an attached
+ * simulation is written by the binding (raw binary + XDMF); otherwise nothing
+ * is written. */
+void io_save_all(gdn_simulation *simulation, char filename[1024], int iternb)
+{
+#ifdef GDN_REF_BOUND
+	if (dg_cuda_attached(simulation)) {
+		if (dg_cuda_save_all(simulation, filename, iternb) != 0)
+			fprintf(stderr, "io_save_all: %s\n", dg_cuda_message());
+		return;
+	}
+#endif
+	(void)simulation;
+	(void)iternb;
+	fprintf(stderr, "io_save_all: %s not written (no HDF5 writer in this build)\n", filename);
+}
 
 typedef struct ref_data {
 	int kind; /* 0 plane wave, 1 PEC cavity, 2 stationary (reference formulas),
@@ -359,3 +380,31 @@ const char *ref_bound_message(void)
 	return dg_cuda_message();
 }
 #endif
+
+/* The reference's own convergence driver utils_l2_time_convergence
+ * (src/utils/convergence.c:43-104) on a msh file: nb_run solves from one
+ * gdn_simulation with dt halved per run; it prints one line per run (error
+ * and order columns, simulation_dump_info, simulation.c:668-692) on stdout.
+ * gpu != 0 (bound library only): every dg_solve of the driver is routed to
+ * the GPU by dg_cuda_route_all(gd) first.  Returns 0, or the routing status. */
+int ref_time_convergence(const char *path, int scheme, const ref_data *d, double init_dt, double tmax,
+						 int nb_run, int gpu, const void *gd)
+{
+	gdn_model model;
+	setup_model(&model, scheme, d);
+#ifdef GDN_REF_BOUND
+	if (gpu && dg_cuda_route_all((const gdn_cuda_data *)gd, NULL) != 0)
+		return -1;
+#else
+	(void)gd;
+	if (gpu)
+		return -2;
+#endif
+	utils_l2_time_convergence(&model, nb_run, path, init_dt, tmax, false);
+	fflush(stdout);
+#ifdef GDN_REF_BOUND
+	if (gpu)
+		dg_cuda_route_all(NULL, NULL);
+#endif
+	return 0;
+}

@@ -102,6 +102,42 @@ def test_d3q4_stationary_data_on_cube_16(msh_files):
     _check(r, g)
 
 
+def test_d3q6_reference_flow_on_cube_8(msh_files):
+    """The d3q6 velocity set (recognised by its get_feq, get_w and get_fR) through the
+    binding, the examples' cos data."""
+    r, g = _pair(msh_files["t4_cube_8"], ref.SCHEME_D3Q6, ref.DATA_EXAMPLE_COS, example_cos_descriptor(),
+                 EXAMPLE_DT, 10)
+    _check(r, g)
+
+
+def test_rk3_metal_boundary_flux_on_cube_16(msh_files):
+    """RK3 with maxwell_num_flux_boundary_metal as the model's boundary flux (the binding maps
+    it to GDN_CUDA_BC_METAL), PEC cavity data, t4_cube_16."""
+    path = msh_files["t4_cube_16"]
+    hmin = ref.RefMesh(path=path).hmin()
+    r, g = _pair(path, ref.SCHEME_RK3_METAL, ref.DATA_CAVITY, capi.cavity_data(), 0.3 * hmin, 30)
+    _check(r, g)
+
+
+@pytest.mark.parametrize("scheme,dt_rule,tmax_steps", [(ref.SCHEME_RK3, "cfl", 20), (ref.SCHEME_D3Q4, "example", 10)])
+def test_reference_convergence_driver_routed_to_the_gpu(msh_files, scheme, dt_rule, tmax_steps):
+    """dg_cuda_route_all, then the reference's own utils_l2_time_convergence
+    (src/utils/convergence.c:43-104) on t4_cube_8.msh: the driver builds its own
+    gdn_simulation and halves dt per run; every dg_solve it makes is attached on first use,
+    attached again when dt changes, and solved on the GPU.  Its printed errors (12
+    decimals) equal those of the unmodified reference's CPU run."""
+    path = msh_files["t4_cube_8"]
+    dt = 0.3 * ref.RefMesh(path=path).hmin() if dt_rule == "cfl" else EXAMPLE_DT
+    d = ref.make_data(kind=ref.DATA_EXAMPLE_COS)
+    cpu = ref.time_convergence(path, scheme, d, dt, tmax_steps * dt, 2, variant="zero")
+    gpu = ref.time_convergence(path, scheme, d, dt, tmax_steps * dt, 2, variant="bound",
+                               gpu_data=example_cos_descriptor())
+    assert len(cpu) == 2 and len(gpu) == 2
+    for a, b in zip(cpu, gpu):
+        assert a["dt"] == b["dt"] and a["iter"] == b["iter"]
+        assert abs(a["error"] - b["error"]) <= 2e-12 + 1e-10 * a["error"], (a, b)
+
+
 def test_rk3_fp32_through_the_binding(msh_files):
     """The precision choice travels through the binding's config."""
     path = msh_files["t4_cube_16"]

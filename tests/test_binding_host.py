@@ -63,3 +63,18 @@ def test_binding_status_of_an_unattached_simulation_is_ok():
     dummy = C.create_string_buffer(256)
     assert L.dg_cuda_attached(dummy) == 0
     assert L.dg_cuda_status(dummy) == 0
+
+
+@needs_bound
+def test_unrouted_convergence_driver_is_the_reference(tmp_path):
+    """The reference's utils_l2_time_convergence in the bound library, nothing routed, prints
+    what the unmodified library prints."""
+    g = np.load(GOLDEN)
+    p = str(tmp_path / "t4_cube_8.msh")
+    kuhn.write_msh22(p, g["t4_cube_8_coords"], g["t4_cube_8_elem2node"])
+    dt = 0.3 * ref.RefMesh(path=p).hmin()
+    d = ref.make_data(kind=ref.DATA_EXAMPLE_COS)
+    a = ref.time_convergence(p, ref.SCHEME_RK3, d, dt, 12 * dt, 2, variant="zero")
+    b = ref.time_convergence(p, ref.SCHEME_RK3, d, dt, 12 * dt, 2, variant="bound")
+    assert len(a) == 2 and [r["iter"] for r in a] == [11, 22]
+    assert [(r["dt"], r["iter"], r["error"]) for r in a] == [(r["dt"], r["iter"], r["error"]) for r in b]
