@@ -242,17 +242,30 @@ int kin_upload_block_tables(const gdn_cuda_tables *t)
 // on [D | I], written at the item's sweep position with theta dt / det.
 // D = I + c Minv F with F = V + sum_outflow s+ E_f S E_f^T, V_ij = -(v . c_ij),
 // row r of Minv F formed directly from the precomputed rows of Minv D_d and
-// Minv E_f S.  Sixteen lanes per item, lane r < 10 holding row r of [D | I] in
-// registers (no local memory): the pivot of column k is found by a shuffle
-// reduction over the rows not yet used (largest |a|, ties to the smallest
-// position), the normalised pivot row is broadcast through shared memory, and
-// every other row eliminates column k.  Rows are not moved: each lane keeps the
-// position its row would have in the row-swapping algorithm, so the pivots are
-// those of the textbook in-place version.  Columns left of the pivot are not
-// updated: they no longer feed a pivot or the inverse.
-constexpr int kBlkThreads = 256; // 16 items per CTA
+// Minv E_f S.  Ten lanes per item, three items per warp (lanes 30 and 31 idle),
+// lane r holding row r of [D | I] in registers (no local memory).
+// - Pivot of column k: the largest |a| among the rows not yet used, ties to the
+//   smallest position.  A shuffle tree over the item's lanes takes the maximum
+//   of |a| as a 64-bit pattern (non-negative doubles order as their bits; +1
+//   keeps every candidate above the rows already used); a ballot names the
+//   lanes that hold it, and only when two do (anywhere in the warp) a second
+//   tree takes the smallest position among them.
+// - The normalised pivot row is broadcast through shared memory, and every
+//   other row eliminates column k.
+// - Rows are not moved: each lane keeps the position its row would have in the
+//   row-swapping algorithm, so the pivots are those of the textbook version.
+// - Columns left of the pivot are not updated: they no longer feed a pivot or
+//   the inverse.
+// - The right half is kept in pivot order: slot t holds the column of the row
+//   that was the pivot at step t.  Before step k only slots 0..k-1 can differ
+//   from the identity (a column of I stays a unit column until its row is a
+//   pivot), so step k updates 9 - k left columns and k + 1 slots, and every
+//   value equals the one the full [D | I] elimination computes.  The slots go
+//   back to their columns when G is written.
+constexpr int kBlkThreads = 256;			  // 8 warps, 24 items per CTA
+constexpr int kBlkItems = kBlkThreads / 32 * 3;
 template <typename GT>
-__global__ void __launch_bounds__(kBlkThreads)
+__global__ void __launch_bounds__(kBlkThreads, 4)
 	kin_blocks_kernel(const double *__restrict__ geom, const double *__restrict__ sown64,
 					  const int *__restrict__ pos, long long ne, KinModel km, double theta,
 					  const int *__restrict__ einst, const double *__restrict__ dt_tab, GT *__restrict__ G,
@@ -260,19 +273,22 @@ __global__ void __launch_bounds__(kBlkThreads)
 					  int *__restrict__ bad)
 {
 	__shared__ double sMD[3][10][10], sMS[4][10][6];
-	__shared__ __align__(16) double sPiv[kBlkThreads / 16][20]; // pivot row of each item
+	__shared__ __align__(16) double sPiv[kBlkItems][20]; // pivot row of each item
 	for (int q = threadIdx.x; q < 300; q += blockDim.x)
 		(&sMD[0][0][0])[q] = (&c_kin_md[0][0][0])[q];
 	for (int q = threadIdx.x; q < 240; q += blockDim.x)
 		(&sMS[0][0][0])[q] = (&c_kin_ms[0][0][0])[q];
 	__syncthreads();
-	const int lane = threadIdx.x & 31, r = lane & 15;
-	double *piv = sPiv[threadIdx.x >> 4];
+	const int lane = threadIdx.x & 31, slot = lane / 10; // slot 3: the two idle lanes
+	const bool row = slot < 3;
+	const int base = 10 * slot, r = lane - base, seg = row ? 10 : 2;
+	const unsigned segmask = row ? 0x3ffu << base : 0xc0000000u;
+	const int witem = (threadIdx.x >> 5) * 3 + (row ? slot : 0);
+	double *piv = sPiv[witem];
 	const long long nu = ne * km.nv;
-	const long long u0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4;
-	const bool item = u0 < nu;
-	const long long u = item ? u0 : nu - 1; // lanes past the end shadow the last item
-	const bool row = r < 10;
+	const long long u0 = blockIdx.x * (long long)kBlkItems + witem;
+	const bool item = row && u0 < nu;
+	const long long u = u0 < nu ? u0 : nu - 1; // lanes past the end shadow the last item
 	const int rr = row ? r : 0;
 	const long long e = u / km.nv;
 	const int v = (int)(u % km.nv);
@@ -296,6 +312,14 @@ __global__ void __launch_bounds__(kBlkThreads)
 		sp[f] = sf > 0.0 ? sf : 0.0;
 	}
 	const double c = theta * dt_tab[einst ? einst[e] : 0] / det;
+	const long long kk = pos[u];
+	if (item && r == 0) { // the item's records (a singular block fails the attach)
+		rcoef[kk] = (GT)c;
+		if (ru64) {
+			ru64[kk] = make_double4(uk[0], uk[1], uk[2], c);
+			rs64[kk] = make_double4(sown64[u * 4], sown64[u * 4 + 1], sown64[u * 4 + 2], sown64[u * 4 + 3]);
+		}
+	}
 	// row rr of [I + c Minv F | I]
 	double a[20];
 #pragma unroll
@@ -308,70 +332,86 @@ __global__ void __launch_bounds__(kBlkThreads)
 				if (f2n(f, jj) == j)
 					acc += sp[f] * sMS[f][rr][jj];
 		a[j] = (rr == j ? 1.0 : 0.0) + c * acc;
-		a[10 + j] = rr == j ? 1.0 : 0.0;
+		a[10 + j] = 0.0; // slot j, filled from step j on
 	}
-	int posn = rr; // this row's position in the row-swapping algorithm
+	int posn = rr;	// this row's position in the row-swapping algorithm
+	unsigned long long col = 0; // 4 bits per step t: the row (= column of I) that was the pivot
 	bool singular = false;
 #pragma unroll
 	for (int k = 0; k < 10; k++) {
 		// pivot: the largest |a[k]| among positions >= k, ties to the smallest position
-		double best = row && posn >= k ? fabs(a[k]) : -1.0;
-		int bkey = (row ? posn : 99) * 32 + lane; // position, then lane
+		const bool cand = row && posn >= k;
+		const unsigned long long val = cand ? (unsigned long long)__double_as_longlong(fabs(a[k])) + 1ull : 0ull;
+		unsigned long long best = val;
 #pragma unroll
-		for (int off = 8; off > 0; off >>= 1) {
-			const double ob = __shfl_xor_sync(0xffffffffu, best, off, 16);
-			const int ok = __shfl_xor_sync(0xffffffffu, bkey, off, 16);
-			if (ob > best || (ob == best && ok < bkey)) {
-				best = ob;
-				bkey = ok;
-			}
+		for (int off = 1; off < 16; off <<= 1) {
+			const int src = r + off < seg ? lane + off : lane;
+			const unsigned long long ob = __shfl_sync(0xffffffffu, best, src);
+			best = ob > best ? ob : best;
 		}
-		const int bpos = bkey >> 5, blane = bkey & 31;
+		best = __shfl_sync(0xffffffffu, best, base);
+		const unsigned win = __ballot_sync(0xffffffffu, val == best) & segmask;
+		int blane = __ffs(win) - 1;
+		if (__any_sync(0xffffffffu, row && (win & (win - 1)) != 0)) { // a tie: the smallest position
+			int key = val == best ? posn * 32 + lane : 0x7fffffff;
+#pragma unroll
+			for (int off = 1; off < 16; off <<= 1) {
+				const int src = r + off < seg ? lane + off : lane;
+				const int ok = __shfl_sync(0xffffffffu, key, src);
+				key = ok < key ? ok : key;
+			}
+			blane = __shfl_sync(0xffffffffu, key, base) & 31;
+		}
+		const int bpos = __shfl_sync(0xffffffffu, posn, blane);
+		col |= (unsigned long long)(blane - base) << (4 * k);
 		// the rows at position k and at the pivot's position trade places
+		const bool pivot = row && lane == blane;
 		if (row && posn == k)
 			posn = bpos;
-		else if (lane == blane)
+		else if (pivot)
 			posn = k;
-		if (lane == blane) {
+		if (pivot) {
 			if (a[k] == 0.0) {
 				singular = true;
 			} else {
 				const double inv = 1.0 / a[k];
 #pragma unroll
-				for (int q = k; q < 20; q++) {
+				for (int q = k + 1; q < 10; q++) {
 					a[q] *= inv;
 					piv[q] = a[q];
 				}
+#pragma unroll
+				for (int t = 0; t < k; t++) {
+					a[10 + t] *= inv;
+					piv[10 + t] = a[10 + t];
+				}
+				a[10 + k] = inv; // 1 x inv
+				piv[10 + k] = inv;
 			}
 		}
-		singular = __shfl_sync(0xffffffffu, (int)singular, blane, 16) != 0 || singular;
+		singular = __shfl_sync(0xffffffffu, (int)singular, blane) != 0 || singular;
 		__syncwarp();
 		const double m = a[k];
 		if (row && lane != blane && m != 0.0) {
 #pragma unroll
-			for (int q = k; q < 20; q++)
+			for (int q = k + 1; q < 10; q++)
 				a[q] -= m * piv[q];
+#pragma unroll
+			for (int t = 0; t <= k; t++)
+				a[10 + t] -= m * piv[10 + t];
 		}
 		__syncwarp(); // the pivot row is read before the next step overwrites it
 	}
-	if (!item || !row)
+	if (!item)
 		return;
 	if (singular) {
 		atomicMax(bad, 1);
 		return;
 	}
-	const long long kk = pos[u];
 	GT *Gk = G + kk * 100 + posn * 10;
 #pragma unroll
-	for (int j = 0; j < 10; j++)
-		Gk[j] = (GT)a[10 + j];
-	if (r == 0) {
-		rcoef[kk] = (GT)c;
-		if (ru64) {
-			ru64[kk] = make_double4(uk[0], uk[1], uk[2], c);
-			rs64[kk] = make_double4(sown64[u * 4], sown64[u * 4 + 1], sown64[u * 4 + 2], sown64[u * 4 + 3]);
-		}
-	}
+	for (int t = 0; t < 10; t++)
+		Gk[(col >> (4 * t)) & 15] = (GT)a[10 + t];
 }
 
 // per-item records of the sweep
@@ -423,7 +463,7 @@ int launch_kin_blocks(const double *geom, const double *sown64, const int *items
 					  double4 *rs64, int *bad, cudaStream_t s)
 {
 	const long long nu = ne * km.nv;
-	kin_blocks_kernel<GT><<<(unsigned)((nu * 16 + kBlkThreads - 1) / kBlkThreads), kBlkThreads, 0, s>>>(
+	kin_blocks_kernel<GT><<<(unsigned)((nu + kBlkItems - 1) / kBlkItems), kBlkThreads, 0, s>>>(
 		geom, sown64, pos, ne, km, theta, einst, dt_tab, G, rcoef, ru64, rs64, bad);
 	GDN_CUDA_TRY(cudaGetLastError());
 	kin_records_kernel<GT><<<(unsigned)((nu + 255) / 256), 256, 0, s>>>(items, pos, sown64, nb, perm, nu, km.nv, rnb,
