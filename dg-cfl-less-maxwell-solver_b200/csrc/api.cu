@@ -602,7 +602,7 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		GDN_TRY(dalloc(h, &h->sown64, 4 * nu));
 		GDN_TRY(dalloc(h, &mask, nu));
 		// upwind masks first: the schedule (and with it the sweep order every
-		// other kinetic array is stored in) is built on the host from them
+		// other kinetic array is stored in) is built on the device from them
 		GDN_TRY(launch_kin_setup<double>(h->face2elem, nf, h->geom64, h->nb, ne, h->km, h->sown64, mask, s));
 		h->launches += 2;
 		GDN_TRY(dalloc(h, &h->items, nu));
@@ -610,9 +610,8 @@ static int attach_impl(gdn_cuda_handle *h, const gdn_cuda_mesh *m, const gdn_cud
 		GDN_TRY(dalloc(h, &h->rnb, nu));
 		GDN_TRY(dalloc(h, &h->rpm, nu));
 		GDN_TRY(dalloc(h, &h->bt, 36LL * nv * (nbf > 0 ? nbf : 1)));
-		long long npasses = 0;
-		GDN_TRY(kin_device_schedule(mask, h->nb, ne, nv, h->items, h->pos, h->level_off, npasses, s));
-		h->launches += npasses + 3;
+		GDN_TRY(kin_device_schedule(mask, h->nb, h->sown64, ne, nv, h->items, h->pos, h->level_off, h->spin_limit, s));
+		h->launches += 4;
 		// state f: FP64 for FP64 and FP32_REFINE, FP32, or BF16
 		if (h->precision == GDN_CUDA_FP64 || h->precision == GDN_CUDA_FP32_REFINE)
 			GDN_TRY(dalloc(h, reinterpret_cast<double **>(&h->f), 60 * nu));

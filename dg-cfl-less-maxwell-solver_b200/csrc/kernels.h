@@ -133,12 +133,13 @@ int kin_build_parts(const int *e2q, const double *node, long long ne, const doub
 					const int *items, long long nitems, int nv, int nparts, const int4 *rnb, int4 *rpm, int *plist,
 					std::vector<int> &plist_host, std::vector<int> &pkey_host, cudaStream_t s);
 
-// Level schedule of the upwind item graph on the device: items[k] (e * nv +
-// v in level order, ascending within a level), pos (its inverse), level_off
-// (host, first item of each level, then the item count); GDN_CUDA_ERR_CYCLE
-// when the graph has a cycle.  npasses = relaxation passes used.
-int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, int nv, int *items, int *pos,
-						std::vector<int> &level_off, long long &npasses, cudaStream_t s);
+// Level schedule of the upwind item graph on the device (Kahn's algorithm by
+// levels, one cooperative launch): items[k] (e * nv + v in level order,
+// ascending within a level), pos (its inverse), level_off (host, first item of
+// each level, then the item count); GDN_CUDA_ERR_CYCLE when the graph has a
+// cycle, GDN_CUDA_ERR_TIMEOUT when a grid barrier waited spin_limit polls.
+int kin_device_schedule(const unsigned char *mask, const int *nb, const double *sown64, long long ne, int nv,
+						int *items, int *pos, std::vector<int> &level_off, long long spin_limit, cudaStream_t s);
 
 // f_eq of the analytic data at the boundary face nodes, t + dt/2 (FP64)
 int launch_kin_boundary_trace(const double *bxyz, long long nbf, const Batch &b, int nv, const double *vi,

@@ -79,35 +79,6 @@ __global__ void kin_mask_kernel(const double *__restrict__ sown64, const int *__
 	mask[u] = m;
 }
 
-// Level schedule on the device.  level(u) = the longest chain of upwind
-// dependencies ending at item u = e * nv + v (the levels Kahn's algorithm
-// yields), by in-place relaxation: each launch raises every level to one
-// more than its highest upwind dependency; levels only grow, and a pass
-// that changes nothing ends the iteration (at most depth + 1 passes).
-__global__ void kin_level_relax_kernel(const unsigned char *__restrict__ mask, const int *__restrict__ nb,
-									   long long ne, int nv, int *level, int *changed)
-{
-	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (u >= ne * nv)
-		return;
-	const unsigned m = mask[u];
-	if (!m)
-		return;
-	const long long e = u / nv;
-	const int v = (int)(u % nv);
-	int l = 0;
-	for (int f = 0; f < 4; f++)
-		if (m >> f & 1) {
-			// other threads raise levels during the pass: read the current value
-			const int d = *(const volatile int *)(level + (long long)nb[e * 4 + f] * nv + v);
-			l = d + 1 > l ? d + 1 : l;
-		}
-	if (l > level[u]) {
-		level[u] = l;
-		*changed = 1;
-	}
-}
-
 __global__ void kin_iota_kernel(int *a, long long n)
 {
 	const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -130,21 +101,27 @@ __global__ void kin_schedule_finish_kernel(const int *__restrict__ items, const 
 		level_off[l + 1] = (int)n;
 }
 
-int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, int nv, int *items, int *pos,
-						std::vector<int> &level_off, long long &npasses, cudaStream_t s)
+static int launch_kin_kahn(const unsigned char *mask, const int *nb, const double *sown64, long long ne, int nv,
+						   int *indeg, int *level, int *front0, int *front1, unsigned *ctl, long long spin_limit,
+						   cudaStream_t s);
+
+int kin_device_schedule(const unsigned char *mask, const int *nb, const double *sown64, long long ne, int nv,
+						int *items, int *pos, std::vector<int> &level_off, long long spin_limit, cudaStream_t s)
 {
 	const long long nu = ne * nv;
 	const unsigned g = (unsigned)((nu + 255) / 256);
-	int *level = nullptr, *lev_sorted = nullptr, *iota = nullptr, *changed = nullptr, *loff = nullptr;
+	int *level = nullptr, *lev_sorted = nullptr, *iota = nullptr, *indeg = nullptr, *loff = nullptr;
+	unsigned *ctl = nullptr;
 	void *tmp = nullptr;
 	size_t tmp_bytes = 0;
 	int rc = GDN_CUDA_OK;
-	int h_changed = 1, maxlev = 0;
+	int maxlev = 0;
 	auto cleanup = [&]() {
 		cudaFree(level);
 		cudaFree(lev_sorted);
 		cudaFree(iota);
-		cudaFree(changed);
+		cudaFree(indeg);
+		cudaFree(ctl);
 		cudaFree(loff);
 		cudaFree(tmp);
 	};
@@ -159,21 +136,27 @@ int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, 
 	GDN_SCHED_TRY(cudaMalloc(&level, nu * sizeof(int)));
 	GDN_SCHED_TRY(cudaMalloc(&lev_sorted, nu * sizeof(int)));
 	GDN_SCHED_TRY(cudaMalloc(&iota, nu * sizeof(int)));
-	GDN_SCHED_TRY(cudaMalloc(&changed, sizeof(int)));
-	GDN_SCHED_TRY(cudaMemsetAsync(level, 0, nu * sizeof(int), s));
-	// a chain longer than the elements of one velocity repeats an element: a cycle
-	npasses = 0;
-	while (h_changed) {
-		if (npasses > ne + 1) {
+	GDN_SCHED_TRY(cudaMalloc(&indeg, nu * sizeof(int)));
+	GDN_SCHED_TRY(cudaMalloc(&ctl, 8 * sizeof(unsigned)));
+	GDN_SCHED_TRY(cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned), s));
+	// levels: Kahn's algorithm, the two frontiers in the sort buffers
+	{
+		const int lrc = launch_kin_kahn(mask, nb, sown64, ne, nv, indeg, level, lev_sorted, iota, ctl, spin_limit, s);
+		if (lrc != GDN_CUDA_OK) {
+			cleanup();
+			return lrc;
+		}
+		unsigned hctl[8];
+		GDN_SCHED_TRY(cudaMemcpyAsync(hctl, ctl, sizeof(hctl), cudaMemcpyDeviceToHost, s));
+		GDN_SCHED_TRY(cudaStreamSynchronize(s));
+		if (hctl[4]) {
+			cleanup();
+			return gdn_set_error(GDN_CUDA_ERR_TIMEOUT, "attach: the level schedule's grid barrier timed out");
+		}
+		if ((long long)hctl[6] != nu) {
 			cleanup();
 			return gdn_set_error(GDN_CUDA_ERR_CYCLE, "attach: the upwind element graph has a cycle");
 		}
-		GDN_SCHED_TRY(cudaMemsetAsync(changed, 0, sizeof(int), s));
-		kin_level_relax_kernel<<<g, 256, 0, s>>>(mask, nb, ne, nv, level, changed);
-		GDN_SCHED_TRY(cudaGetLastError());
-		GDN_SCHED_TRY(cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, s));
-		GDN_SCHED_TRY(cudaStreamSynchronize(s));
-		npasses++;
 	}
 	kin_iota_kernel<<<g, 256, 0, s>>>(iota, nu);
 	GDN_SCHED_TRY(cudaGetLastError());
@@ -181,7 +164,7 @@ int kin_device_schedule(const unsigned char *mask, const int *nb, long long ne, 
 	// ascending e * nv + v, as the host schedule had it
 	int bits = 1;
 	{
-		int *dmax = changed;
+		int *dmax = reinterpret_cast<int *>(ctl + 7);
 		GDN_SCHED_TRY(cub::DeviceReduce::Max(nullptr, tmp_bytes, level, dmax, (int)nu, s));
 		GDN_SCHED_TRY(cudaMalloc(&tmp, tmp_bytes));
 		GDN_SCHED_TRY(cub::DeviceReduce::Max(tmp, tmp_bytes, level, dmax, (int)nu, s));
@@ -820,6 +803,129 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
 	}
 	__syncthreads();
 	return s_ok != 0;
+}
+
+// Level schedule by Kahn's algorithm, one level per grid barrier, in one
+// cooperative launch.  indeg[u] = the upwind dependencies of item u not yet
+// placed; the items of level l are listed in one frontier, and placing one
+// releases its downwind items (across the faces it flows out of: s > 0 there,
+// s < 0 on the other side, so each dependency edge is counted once on each
+// end).  An item whose last dependency is placed at level l enters level
+// l + 1, so level(u) = the longest upwind chain ending at u.  ctl: [0] barrier
+// arrivals, [1..3] frontier sizes of levels l mod 3, [4] error, [5] levels,
+// [6] items placed (fewer than all: a cycle).
+constexpr int kKahnThreads = 256;
+__global__ void __launch_bounds__(kKahnThreads)
+	kin_kahn_kernel(const unsigned char *__restrict__ mask, const int *__restrict__ nb,
+					const double *__restrict__ sown64, long long ne, int nv, int *__restrict__ indeg,
+					int *__restrict__ level, int *front0, int *front1, unsigned *ctl, long long spin_limit)
+{
+	const long long nu = ne * nv;
+	const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	const long long nthreads = (long long)gridDim.x * blockDim.x;
+	const int lane = threadIdx.x & 31;
+	const unsigned lt = (1u << lane) - 1u;
+	unsigned *bar = ctl, *cnt = ctl + 1;
+	int *err = reinterpret_cast<int *>(ctl + 4);
+	// level 0: the items without upwind dependencies (warp-aggregated appends)
+	for (long long b = tid - lane; b < nu; b += nthreads) {
+		const long long u = b + lane;
+		int d = 0;
+		if (u < nu) {
+			d = __popc(mask[u]);
+			indeg[u] = d;
+		}
+		const bool push = u < nu && d == 0;
+		const unsigned bal = __ballot_sync(0xffffffffu, push);
+		unsigned base = 0;
+		if (lane == 0 && bal)
+			base = atomicAdd(cnt, __popc(bal));
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (push) {
+			front0[base + __popc(bal & lt)] = (int)u;
+			level[u] = 0;
+		}
+	}
+	if (!grid_barrier(bar, gridDim.x, err, spin_limit))
+		return;
+	int *cur = front0, *nxt = front1;
+	long long placed = 0;
+	int l = 0;
+	for (;; l++) {
+		const unsigned n = *(volatile unsigned *)(cnt + l % 3);
+		if (n == 0)
+			break;
+		placed += n;
+		if (tid == 0)
+			cnt[(l + 2) % 3] = 0; // level l - 1's size: read by every CTA before the last barrier
+		for (long long b = tid - lane; b < n; b += nthreads) {
+			const long long i = b + lane;
+			const long long u = i < n ? cur[i] : 0;
+			const long long e = u / nv;
+			const int v = (int)(u % nv);
+#pragma unroll
+			for (int f = 0; f < 4; f++) {
+				bool push = false;
+				int w = 0;
+				if (i < n) {
+					const int we = nb[e * 4 + f];
+					if (we >= 0 && sown64[u * 4 + f] > 0.0) {
+						w = (int)((long long)we * nv + v);
+						push = atomicSub(indeg + w, 1) == 1;
+					}
+				}
+				const unsigned bal = __ballot_sync(0xffffffffu, push);
+				unsigned base = 0;
+				if (lane == 0 && bal)
+					base = atomicAdd(cnt + (l + 1) % 3, __popc(bal));
+				base = __shfl_sync(0xffffffffu, base, 0);
+				if (push) {
+					nxt[base + __popc(bal & lt)] = w;
+					level[w] = l + 1;
+				}
+			}
+		}
+		if (!grid_barrier(bar, (unsigned)(l + 2) * gridDim.x, err, spin_limit))
+			return;
+		int *t = cur;
+		cur = nxt;
+		nxt = t;
+	}
+	if (tid == 0) {
+		ctl[5] = (unsigned)l;
+		ctl[6] = (unsigned)placed;
+	}
+}
+
+// cooperative launch of kin_kahn_kernel with every CTA resident
+static int launch_kin_kahn(const unsigned char *mask, const int *nb, const double *sown64, long long ne, int nv,
+						   int *indeg, int *level, int *front0, int *front1, unsigned *ctl, long long spin_limit,
+						   cudaStream_t s)
+{
+	int dev = 0, nsm = 0, per = 0;
+	GDN_CUDA_TRY(cudaGetDevice(&dev));
+	GDN_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+	GDN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kin_kahn_kernel, kKahnThreads, 0));
+	const long long nu = ne * nv;
+	long long grid = (long long)nsm * per;
+	const long long need = (nu + kKahnThreads - 1) / kKahnThreads;
+	if (grid > need)
+		grid = need;
+	if (grid < 1)
+		grid = 1;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3((unsigned)grid);
+	cfg.blockDim = dim3(kKahnThreads);
+	cfg.stream = s;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	GDN_CUDA_TRY(cudaLaunchKernelEx(&cfg, kin_kahn_kernel, mask, nb, sown64, ne, nv, indeg, level, front0, front1,
+									ctl, spin_limit));
+	GDN_CUDA_TRY(cudaGetLastError());
+	return GDN_CUDA_OK;
 }
 
 // All levels of one transport solve in one cooperative launch: the CTAs walk
