@@ -814,7 +814,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned target, i
 // l + 1, so level(u) = the longest upwind chain ending at u.  ctl: [0] barrier
 // arrivals, [1..3] frontier sizes of levels l mod 3, [4] error, [5] levels,
 // [6] items placed (fewer than all: a cycle).
-constexpr int kKahnThreads = 256;
+constexpr int kKahnThreads = 512; // one CTA per SM: the barrier's arrivals, not the work, set a level's time
 __global__ void __launch_bounds__(kKahnThreads)
 	kin_kahn_kernel(const unsigned char *__restrict__ mask, const int *__restrict__ nb,
 					const double *__restrict__ sown64, long long ne, int nv, int *__restrict__ indeg,
@@ -906,8 +906,10 @@ static int launch_kin_kahn(const unsigned char *mask, const int *nb, const doubl
 	GDN_CUDA_TRY(cudaGetDevice(&dev));
 	GDN_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
 	GDN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kin_kahn_kernel, kKahnThreads, 0));
+	if (per < 1)
+		return gdn_set_error(GDN_CUDA_ERR_CUDA, "attach: the level schedule kernel cannot be resident");
 	const long long nu = ne * nv;
-	long long grid = (long long)nsm * per;
+	long long grid = nsm;
 	const long long need = (nu + kKahnThreads - 1) / kKahnThreads;
 	if (grid > need)
 		grid = need;
