@@ -990,8 +990,9 @@ __device__ __forceinline__ bool wait_ready(const int *flag, int *err, long long 
 // instead of a barrier per level.  chunks[] lists the solve's 32-item chunks
 // in sweep order, never straddling a level, so every upwind item of a chunk
 // lies in an earlier chunk.  Each CTA takes the next chunk from an atomic
-// counter, stages it, waits (acquire) only for the flags of its own items'
-// upwind neighbours, solves, and publishes its items' flags (release).  A
+// counter, stages it, waits (acquire, warp 0 only: a barrier then orders
+// the other warps' loads) for the flags of its own items' upwind neighbours,
+// solves, and publishes its items' flags (release).  A
 // chunk waits only on chunks taken earlier by CTAs already running, so the
 // solve progresses with any number of resident CTAs; the critical path is the
 // longest upwind chain, not the level count times a launch.  A CTA takes its
@@ -1025,12 +1026,15 @@ __global__ void __launch_bounds__(kSwThreads)
 		const int2 ck = chunks[c];
 		sweep_chunk<F, Y, T, ACC, BD, SPARSE, true, false>(
 			p, ck.x, ck.y, gsh, [&](const int *nbk, const int *, bool act) {
-				if (!act)
-					return;
+				// warp 0 waits for the chunk; the barrier orders the other
+				// warps' trace loads after its acquires
+				if (threadIdx.x < 32 && act) {
 #pragma unroll
-				for (int f = 0; f < 4; f++)
-					if (nbk[f] >= 0 && !wait_ready(ready + nbk[f], err, spin_limit))
-						s_fail = 1;
+					for (int f = 0; f < 4; f++)
+						if (nbk[f] >= 0 && !wait_ready(ready + nbk[f], err, spin_limit))
+							s_fail = 1;
+				}
+				__syncthreads();
 			});
 		// sweep_chunk ended with a barrier after every thread's y stores
 		if (s_fail)
@@ -1073,12 +1077,13 @@ __global__ void __launch_bounds__(kSwThreads)
 		sweep_chunk<F, Y, T, ACC, BD, SPARSE, true, false>(
 			p, ck.x, ck.x + ck.y, gsh,
 			[&](const int *nbk, const int *pmk, bool act) {
-				if (!act)
-					return;
+				if (threadIdx.x < 32 && act) {
 #pragma unroll
-				for (int f = 0; f < 4; f++)
-					if (nbk[f] >= 0 && (pmk[f] & kPartExternal) && !wait_ready(ready + nbk[f], err, spin_limit))
-						s_fail = 1;
+					for (int f = 0; f < 4; f++)
+						if (nbk[f] >= 0 && (pmk[f] & kPartExternal) && !wait_ready(ready + nbk[f], err, spin_limit))
+							s_fail = 1;
+				}
+				__syncthreads();
 			},
 			plist);
 		// sweep_chunk ended with a barrier after every thread's y stores
