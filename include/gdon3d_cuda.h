@@ -327,7 +327,10 @@ int gdn_cuda_kin_sweep_mode(gdn_cuda_handle *h, int *mode);
  * state back (get_state, solve, step_host, error_l2, save_xdmf) then returns
  * GDN_CUDA_ERR_TIMEOUT and the state is invalid until it is set again.
  * Default 2^21 polls (about a second); 0 gives up at the first poll that
- * finds its condition unmet.  Captured step loops are rebuilt. */
+ * finds its condition unmet.  Captured step loops are rebuilt.  The kinetic
+ * attach's level schedule (one cooperative launch with a grid barrier per
+ * level) always waits with the default; when it runs out, the attach returns
+ * GDN_CUDA_ERR_TIMEOUT. */
 int gdn_cuda_set_wait_limit(gdn_cuda_handle *h, long long polls);
 /* RK3: the stage-kernel variant in use (1 or 2, see rk3_variant; 0 for the
  * kinetic scheme) and the resident CTAs per SM it was compiled for (may be
