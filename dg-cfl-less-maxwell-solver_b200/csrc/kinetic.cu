@@ -961,29 +961,49 @@ __global__ void __launch_bounds__(kSwThreads) kin_levels_kernel(KinSweepParams p
 	}
 }
 
-// Bounded wait for an upwind item's readiness flag (acquire): true once it is
-// set; false when *err is set by another CTA, or after spin_limit further
-// polls (then *err is set here), so a lost producer ends the launch instead
-// of hanging it.  (Relaxed polls followed by one acquire fence per thread
-// measured slower on B200: 5.4 vs 4.8 ms per 64^3 FP32 step.)
-__device__ __forceinline__ bool wait_ready(const int *flag, int *err, long long spin_limit)
+// Bounded wait for the readiness flags of an item's upwind neighbours
+// (need[f]): the flags are polled together with relaxed loads, and once all
+// are set one acquire fence orders the caller's later loads after the
+// producers' releases (the acquire pattern).  false when *err is set by
+// another CTA, or after spin_limit further polls (then *err is set here), so
+// a lost producer ends the launch instead of hanging it.  Only warp 0 of a CTA
+// waits; acquire loads one flag after another cost up to three L2 round trips
+// when the flags are already set.
+__device__ __forceinline__ bool wait_ready_all(const int *ready, const int nbk[4], const bool need[4], int *err,
+											   long long spin_limit)
 {
-	int v;
-	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-	if (v)
-		return true;
+	bool ok[4];
+#pragma unroll
+	for (int f = 0; f < 4; f++)
+		ok[f] = !need[f];
 	const volatile int *verr = err;
-	for (long long it = 0; it < spin_limit; it++) {
+	for (long long it = 0;; it++) {
+		int v[4];
+#pragma unroll
+		for (int f = 0; f < 4; f++) {
+			v[f] = 1;
+			if (!ok[f])
+				asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v[f]) : "l"(ready + nbk[f]) : "memory");
+		}
+		bool all = true;
+#pragma unroll
+		for (int f = 0; f < 4; f++) {
+			ok[f] = ok[f] || v[f] != 0;
+			all = all && ok[f];
+		}
+		if (all)
+			break;
 		if (*verr)
 			return false;
-		if (it >= 32) // back off once the producer is evidently not about to finish
+		if (it >= spin_limit) {
+			atomicExch(err, 1);
+			return false;
+		}
+		if (it >= 32)
 			__nanosleep(32);
-		asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-		if (v)
-			return true;
 	}
-	atomicExch(err, 1);
-	return false;
+	asm volatile("fence.acq_rel.gpu;" ::: "memory");
+	return true;
 }
 
 // The whole transport solve in one launch, driven by per-item readiness flags
@@ -1029,10 +1049,12 @@ __global__ void __launch_bounds__(kSwThreads)
 				// warp 0 waits for the chunk; the barrier orders the other
 				// warps' trace loads after its acquires
 				if (threadIdx.x < 32 && act) {
+					bool need[4];
 #pragma unroll
 					for (int f = 0; f < 4; f++)
-						if (nbk[f] >= 0 && !wait_ready(ready + nbk[f], err, spin_limit))
-							s_fail = 1;
+						need[f] = nbk[f] >= 0;
+					if (!wait_ready_all(ready, nbk, need, err, spin_limit))
+						s_fail = 1;
 				}
 				__syncthreads();
 			});
@@ -1078,10 +1100,12 @@ __global__ void __launch_bounds__(kSwThreads)
 			p, ck.x, ck.x + ck.y, gsh,
 			[&](const int *nbk, const int *pmk, bool act) {
 				if (threadIdx.x < 32 && act) {
+					bool need[4];
 #pragma unroll
 					for (int f = 0; f < 4; f++)
-						if (nbk[f] >= 0 && (pmk[f] & kPartExternal) && !wait_ready(ready + nbk[f], err, spin_limit))
-							s_fail = 1;
+						need[f] = nbk[f] >= 0 && (pmk[f] & kPartExternal);
+					if (!wait_ready_all(ready, nbk, need, err, spin_limit))
+						s_fail = 1;
 				}
 				__syncthreads();
 			},
