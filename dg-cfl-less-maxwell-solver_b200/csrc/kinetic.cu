@@ -1449,7 +1449,11 @@ int kin_flags_grid(int device, int acc, int sparse, int *grid)
 			 : acc == 1 ? (const void *)kin_flags_kernel<F, Y, T, 1, true, false>
 						: (const void *)kin_flags_kernel<F, Y, T, 2, false, false>;
 	GDN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kSwThreads, 0));
-	*grid = nsm * (per > 0 ? per : 1);
+	// at most 4 CTAs per SM: the chunks in flight then poll and publish least
+	// against each other (64^3 FP32 ms per step for 2 to 6 CTAs per SM: 5.20,
+	// 4.56, 4.35, 4.46, 4.54)
+	const int cap = 4;
+	*grid = nsm * (per > cap ? cap : (per > 0 ? per : 1));
 	return GDN_CUDA_OK;
 }
 
