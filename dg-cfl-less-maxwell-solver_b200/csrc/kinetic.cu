@@ -1473,7 +1473,10 @@ int kin_levels_grid(int device, int acc, int sparse, int *grid)
 			 : acc == 1 ? (const void *)kin_levels_kernel<F, Y, T, 1, true, false>
 						: (const void *)kin_levels_kernel<F, Y, T, 2, false, false>;
 	GDN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kSwThreads, 0));
-	*grid = nsm * per;
+	// at most 3 CTAs per SM, about one per 32-item chunk of a 64^3 level: fewer
+	// arrivals per grid barrier (64^3 FP32 ms per step for 2 / 3 / 4 CTAs per
+	// SM: 6.04, 5.81, 6.75)
+	*grid = nsm * (per > 3 ? 3 : per);
 	return GDN_CUDA_OK;
 }
 
