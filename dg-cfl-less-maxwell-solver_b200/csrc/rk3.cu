@@ -816,7 +816,11 @@ static void launch_rk3_one(const Rk3Params<T> &pin, int variant, cudaStream_t s)
 	typedef Rk3Variants<T> V;
 	Rk3Params<T> p = pin;
 	// L2 prefetch distance: the CTAs resident on the GPU at this variant's cap
-	p.l2_ahead = p.l2_ahead ? p.num_sms * (variant == 0 ? V::lo : V::hi) : 0;
+	// (FP32), half of them (FP64).  96^3 ms per step, FP32 / FP64, for none,
+	// half, one and two times the resident CTAs: 4.35 / 9.45, 4.25 / 9.03,
+	// 4.24 / 9.14, 4.32 / 9.67.
+	const int resident = p.num_sms * (variant == 0 ? V::lo : V::hi);
+	p.l2_ahead = p.l2_ahead ? (sizeof(T) == 8 ? resident / 2 : resident) : 0;
 	const unsigned nblk = (unsigned)((p.ne + 31) / 32);
 	const int sm = rk3_smem_bytes<T, FA>();
 	if (variant == 0)
